@@ -1,0 +1,462 @@
+#!/usr/bin/env python
+"""Batched fp-NTT product throughput on B200.
+
+Workload (one "step"): 10,000 independent products whose larger operand has
+log-uniform limb count in [152, 65536], size ratio (smaller/larger) uniform in
+[0.25, 1], 20% squarings, limbs uniform random uint64 with the top limb
+nonzero, seeded (numpy PCG64).  The whole batch runs as one replay of the
+engine's CUDA graph (one work-queue launch per pipeline step); every step's
+operands (~0.7 GB) and workspace (~9 GB) are far larger than the 126 MB L2.
+
+Printed JSON line (rank 0):
+  value     output limbs/s, batch replay with operands resident in HBM
+  e2e       same metric through nbg_mul_batch (host buffers; H2D + D2H inside)
+  unbatched the same products issued one per call (nbg_mul_batch_dev, count 1)
+  roofline  dominant kernel's algorithmic FP64 instructions / its measured
+            duration, against the FP64 issue rate measured in this run
+  cpu_baseline  the CPU oracle (restatement of the reference) on the host cores
+
+--impl reference times the reference's CPU algorithm (the oracle port; Julia
+is not available on this machine) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "nativebigint.jl_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "batched fp-NTT mul output limbs/s vs unbatched GPU mul, bit-exact; p50/p99 ms"
+WORKLOAD = "10,000 mixed products: larger operand log-uniform [152, 65536] limbs, ratio U[0.25,1], 20% squares"
+
+
+# ---------------------------------------------------------------------------
+# workload
+
+def gen_workload(seed: int, count: int):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    m = np.exp(rng.uniform(math.log(152), math.log(65536), count)).astype(np.int64)
+    ratio = rng.uniform(0.25, 1.0, count)
+    n = np.maximum(1, np.round(m * ratio).astype(np.int64))
+    sq = rng.random(count) < 0.2
+    n = np.where(sq, m, n)
+    # operand limbs, one flat array: a_k then (for products) b_k
+    la = m.copy()
+    lb = np.where(sq, 0, n)
+    off_a = np.zeros(count, dtype=np.int64)
+    off_b = np.zeros(count, dtype=np.int64)
+    pos = 0
+    for k in range(count):
+        off_a[k] = pos
+        pos += int(la[k])
+        off_b[k] = pos
+        pos += int(lb[k])
+    limbs = rng.integers(0, 2**64, pos, dtype=np.uint64, endpoint=False)
+    for top in (off_a + la - 1, (off_b + lb - 1)[~sq]):  # top limbs nonzero
+        limbs[top] = np.where(limbs[top] == 0, np.uint64(1), limbs[top])
+    out_off = np.concatenate([[0], np.cumsum(m + n)[:-1]]).astype(np.int64)
+    return dict(m=m, n=n, sq=sq, off_a=off_a, off_b=off_b, limbs=limbs, out_off=out_off,
+                out_total=int((m + n).sum()))
+
+
+def bits_of(limbs: np.ndarray, off: int, ln: int) -> int:
+    return 64 * (ln - 1) + int(limbs[off + ln - 1]).bit_length()
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU side (oracle = restatement of the reference; test infrastructure)
+
+def cpu_rate(W, idx: list[int], threads: int) -> tuple[float, float]:
+    """Runs the oracle on products idx with `threads` host threads; returns
+    (output limbs/s, seconds).  ctypes releases the GIL during the C call."""
+    import oracle
+
+    L = oracle.lib()
+    limbs = W["limbs"]
+    # plans first (the oracle's plan cache is filled single-threaded)
+    for k in idx:
+        ba = bits_of(limbs, W["off_a"][k], W["m"][k])
+        bb = ba if W["sq"][k] else bits_of(limbs, W["off_b"][k], W["n"][k])
+        _, N = oracle.ntt_params(ba, bb)
+        L.orc_plan_get(N, 0)
+        L.orc_plan_get(N, 1)
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    base = limbs.ctypes.data
+    outs = {k: np.empty(int(W["m"][k] + W["n"][k]), dtype=np.uint64) for k in idx}
+
+    def one(k):
+        m, n = int(W["m"][k]), int(W["n"][k])
+        pa = ctypes.cast(base + 8 * int(W["off_a"][k]), u64p)
+        r = outs[k].ctypes.data_as(u64p)
+        if W["sq"][k]:
+            L.orc_sqr_fpntt2(r, pa, m)
+        else:
+            pb = ctypes.cast(base + 8 * int(W["off_b"][k]), u64p)
+            L.orc_mul_fpntt2(r, pa, m, pb, n)
+        return m + n
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        total = sum(ex.map(one, sorted(idx, key=lambda k: -int(W["m"][k] + W["n"][k]))))
+    dt = time.perf_counter() - t0
+    return total / dt, dt
+
+
+def cpu_sample(W, budget_s: float, threads: int) -> tuple[list[int], str]:
+    """A bounded prefix of the workload sized for ~budget_s of CPU work."""
+    # single-thread cost model: ~4.5e-7 s per output limb for this size mix (oracle, scalar)
+    per = 4.5e-7
+    tot, idx = 0.0, []
+    for k in range(len(W["m"])):
+        c = per * float(W["m"][k] + W["n"][k])
+        if idx and tot + c > budget_s * threads:
+            break
+        idx.append(k)
+        tot += c
+    return idx, f"first {len(idx)} of the {len(W['m'])} products (same seed), {threads} threads"
+
+
+# ---------------------------------------------------------------------------
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    W = gen_workload(args.seed, args.products)
+    threads = os.cpu_count() or 1
+    idx, desc = cpu_sample(W, args.cpu_seconds / max(1, args.steps + args.warmup) * 3, threads)
+    for _ in range(args.warmup):
+        cpu_rate(W, idx[: max(1, len(idx) // 4)], threads)
+    rates, times = [], []
+    for _ in range(args.steps):
+        r, dt = cpu_rate(W, idx, threads)
+        rates.append(r)
+        times.append(dt)
+    value = float(statistics.median(rates))
+    out_limbs = int(sum(int(W["m"][k] + W["n"][k]) for k in idx))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "output limbs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "products": args.products, "seed": args.seed,
+                   "sample_products": len(idx), "sample_output_limbs": out_limbs},
+        "cpu_baseline": {"value": value, "unit": "output limbs/s", "cores": threads, "kind": "port",
+                         "sample": desc + "; CPU restatement of src/fpntt.jl (Julia is not installed)"},
+        "e2e": {"value": value, "unit": "output limbs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def fp64_peak() -> dict:
+    path = os.path.join(ROOT, "nativebigint.jl_b200", "lib", "libnbgpu_peak.so")
+    L = ctypes.CDLL(path)
+    L.nbgpeak_fp64.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    fma, add = ctypes.c_double(), ctypes.c_double()
+    import torch
+
+    rc = L.nbgpeak_fp64(torch.cuda.current_device(), ctypes.byref(fma), ctypes.byref(add))
+    if rc:
+        raise RuntimeError("fp64 peak probe failed")
+    return {"dfma_per_s": fma.value, "dadd_per_s": add.value}
+
+
+def traffic_from_profiles(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(kernel, {}).get("bytes_per_launch_full_batch")
+    except (OSError, ValueError):
+        return None
+
+
+def run_ours(args, rank: int, world: int) -> None:
+    import torch
+    import torch.distributed as dist
+
+    import nbgpu
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    nbgpu._check(nbgpu.lib().nbg_init(dev))
+    stream = torch.cuda.Stream()
+    W = gen_workload(args.seed + rank, args.products)
+    count = args.products
+    limbs = W["limbs"]
+    d_in = torch.from_numpy(limbs).to(f"cuda:{dev}")
+    d_out = torch.zeros(W["out_total"], dtype=torch.uint64, device=f"cuda:{dev}")
+    ib, ob = d_in.data_ptr(), d_out.data_ptr()
+    items = []
+    for k in range(count):
+        m, n, sq = int(W["m"][k]), int(W["n"][k]), bool(W["sq"][k])
+        ba = bits_of(limbs, int(W["off_a"][k]), m)
+        bb = ba if sq else bits_of(limbs, int(W["off_b"][k]), n)
+        items.append((ob + 8 * int(W["out_off"][k]), ib + 8 * int(W["off_a"][k]),
+                      None if sq else ib + 8 * int(W["off_b"][k]), m, n, ba, bb))
+    descs = nbgpu.make_descs(items)
+    torch.cuda.synchronize()
+    bt = nbgpu.Batch(descs)
+    out_limbs = W["out_total"]
+    s = stream.cuda_stream
+
+    # warm-up
+    for _ in range(args.warmup):
+        bt.run(s)
+    torch.cuda.synchronize()
+
+    # timed region: K replays of the whole batch
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = nbgpu.launch_count()
+    with ClockSampler(dev) as clk:
+        with torch.cuda.stream(stream):
+            evs[0].record(stream)
+            for i in range(args.steps):
+                bt.run(s)
+                evs[i + 1].record(stream)
+        torch.cuda.synchronize()
+    launches = nbgpu.launch_count() - l0
+    if world > 1:
+        dist.barrier()
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    total_ms = evs[0].elapsed_time(evs[-1])
+    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
+    units = torch.tensor([float(out_limbs) * args.steps], dtype=torch.float64, device=f"cuda:{dev}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(units, op=dist.ReduceOp.SUM)
+    total_ms_max = float(t.item())
+    value = float(units.item()) / (total_ms_max / 1e3)
+
+    # bit-exactness of this run's results: a seeded sample against GMP
+    import oracle
+
+    res = d_out.cpu().numpy()
+    chk = np.random.default_rng(5).choice(count, min(args.check, count), replace=False)
+    bad = 0
+    for k in chk:
+        m, n = int(W["m"][k]), int(W["n"][k])
+        a = limbs[W["off_a"][k]: W["off_a"][k] + m]
+        want = oracle.gmp_sqr(a) if W["sq"][k] else oracle.gmp_mul(a, limbs[W["off_b"][k]: W["off_b"][k] + n])
+        got = res[W["out_off"][k]: W["out_off"][k] + m + n]
+        bad += int(not np.array_equal(got, want))
+    if bad:
+        raise SystemExit(f"bench: {bad} of {len(chk)} checked products differ from GMP")
+
+    line = None
+    if rank == 0:
+        # per-launch live timing (CUDA events between launches, same stream)
+        stats = bt.stats()
+        prof = [bt.profile(s) for _ in range(3)]
+        avg = [statistics.mean(p[i] for p in prof) for i in range(len(stats))]
+        kern = {}
+        for st_, ms in zip(stats, avg):
+            d = kern.setdefault(st_["kind"], {"ms": 0.0, "ops": 0.0, "bytes": 0.0, "launches": 0})
+            d["ms"] += ms
+            d["ops"] += st_["alg_ops"]
+            d["bytes"] += st_["alg_bytes"]
+            d["launches"] += 1
+        dom = max(kern, key=lambda k: kern[k]["ms"])
+        D = kern[dom]
+        peak = fp64_peak()
+        achieved = D["ops"] / (D["ms"] / 1e3) / 1e12
+        pk = peak["dfma_per_s"] / 1e12
+        tot_ops = sum(st_["alg_ops"] for st_ in stats)
+        roof = {
+            "bound": "fp64", "kernel": dom, "achieved": achieved, "peak": pk, "unit": "T FP64 instr/s",
+            "frac": achieved / pk, "traffic": traffic_from_profiles(dom),
+            "peak_source": "measured: DFMA issue rate of libnbgpu_peak.so in this run (MEASURED_PEAKS.json has no FP64 figure)",
+            "alg_ops_per_launch": D["ops"] / D["launches"], "ms_per_launch": D["ms"] / D["launches"],
+            "hbm": {"alg_bytes_per_launch": D["bytes"] / D["launches"],
+                    "achieved_gbs": D["bytes"] / (D["ms"] / 1e3) / 1e9, "peak_gbs": 6542.7,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "kernels": {k: {"ms_per_step": v["ms"], "share": v["ms"] / sum(x["ms"] for x in kern.values()),
+                            "alg_tops": v["ops"] / (v["ms"] / 1e3) / 1e12 if v["ms"] else 0.0}
+                        for k, v in kern.items()},
+            "batch_alg_tops": tot_ops / (statistics.median(step_ms) / 1e3) / 1e12,
+        }
+
+        # unbatched: the same products one call each (device buffers)
+        lat = []
+        nb = min(args.unbatched, count)
+        one = (nbgpu.NbgDesc * 1)()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ul = 0
+        for k in range(nb):
+            one[0] = descs[k]
+            c0 = time.perf_counter()
+            nbgpu.mul_batch_dev(one, s)
+            lat.append(1e3 * (time.perf_counter() - c0))
+            ul += int(W["m"][k] + W["n"][k])
+        torch.cuda.synchronize()
+        un_s = time.perf_counter() - t0
+        unbatched = {"value": ul / un_s, "unit": "output limbs/s", "products": nb,
+                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "products_per_s": nb / un_s}
+
+        # e2e: host buffers through nbg_mul_batch (pinned), copies inside the call
+        pin_in = torch.from_numpy(limbs).pin_memory()
+        pin_out = torch.zeros(W["out_total"], dtype=torch.uint64).pin_memory()
+        hib, hob = pin_in.data_ptr(), pin_out.data_ptr()
+        hitems = []
+        for k in range(count):
+            m, n, sq = int(W["m"][k]), int(W["n"][k]), bool(W["sq"][k])
+            hitems.append((hob + 8 * int(W["out_off"][k]), hib + 8 * int(W["off_a"][k]),
+                           None if sq else hib + 8 * int(W["off_b"][k]), m, n, 0, 0))
+        hdescs = nbgpu.make_descs(hitems)
+        L = nbgpu.lib()
+        for _ in range(1):
+            nbgpu._check(L.nbg_mul_batch(ctypes.cast(hdescs, ctypes.c_void_p), count))
+        e2e_t = []
+        for _ in range(max(2, min(args.steps, 5))):
+            t0 = time.perf_counter()
+            nbgpu._check(L.nbg_mul_batch(ctypes.cast(hdescs, ctypes.c_void_p), count))
+            e2e_t.append(time.perf_counter() - t0)
+        e2e_val = out_limbs / statistics.median(e2e_t)
+        if not np.array_equal(pin_out.numpy(), res):
+            raise SystemExit("bench: e2e results differ from the device-resident batch")
+
+        # CPU baseline on a bounded sample
+        threads = os.cpu_count() or 1
+        idx, desc = cpu_sample(W, args.cpu_seconds, threads)
+        cpu_v, _ = cpu_rate(W, idx, threads)
+
+        clocks = clk.summary()
+        med = statistics.median(step_ms)
+        line = {
+            "metric": METRIC, "value": value, "unit": "output limbs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "products": count, "seed": args.seed,
+                       "output_limbs_per_step": out_limbs, "l2": "inputs larger than L2 (0.7 GB operands, 9 GB workspace)",
+                       "parallelism": f"batch shards x{world}, no collective"},
+            "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+            "products_per_s": count * world / (total_ms_max / args.steps / 1e3),
+            "vs_unbatched": value / world / unbatched["value"],
+            "unbatched": unbatched,
+            "bitexact": {"checked_vs_gmp": int(len(chk)), "mismatches": bad},
+            "e2e": {"value": e2e_val, "unit": "output limbs/s",
+                    "h2d_bytes_per_step": int(8 * len(limbs)), "d2h_bytes_per_step": int(8 * out_limbs)},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "roofline": roof,
+            "cpu_baseline": {"value": cpu_v, "unit": "output limbs/s", "cores": threads, "kind": "port",
+                             "sample": desc + "; CPU restatement of src/fpntt.jl (Julia is not installed)"},
+            "median_step_ms": med,
+        }
+        print(json.dumps(line), flush=True)
+    bt.close()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--products", type=int, default=10000)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--check", type=int, default=64, help="products verified against GMP after timing")
+    ap.add_argument("--unbatched", type=int, default=10000, help="products issued one per call")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,145 @@
+/*
+ * nbgpu.h — C ABI of the B200 fp-NTT multiplication engine (libnbgpu.so).
+ *
+ * Drop-in for the two-prime Float64 NTT branch of NativeBigInt.jl's mpn
+ * multiply: every product is bit-identical to the reference's
+ * mul_fpntt2!/sqr_fpntt2! (src/fpntt.jl:982-1037).  Plain pointers and sizes
+ * only; limbs are little-endian uint64_t.  All entry points return an int
+ * status (NBG_OK = 0) and never abort; nbg_last_error() describes the last
+ * failure on the calling thread.  The library is thread-safe: calls on one
+ * device are serialized by an internal lock.
+ */
+#ifndef NBGPU_H
+#define NBGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define NBG_OK 0
+#define NBG_EINVAL 1   /* bad argument (null pointer, n < 1, aliasing, ...) */
+#define NBG_ERANGE 2   /* transform length beyond 315*2^34: the reference's ArgumentError (fpntt.jl:948-949) */
+#define NBG_ENOMEM 3   /* device or host allocation failed / over the HBM budget */
+#define NBG_ECUDA 4    /* CUDA runtime error */
+#define NBG_ETIMEOUT 5 /* a bounded wait expired */
+#define NBG_EBUSY 6    /* queue full (serving back-pressure) */
+#define NBG_ENODEV 7   /* no CUDA device */
+
+/* ---- products, host buffers (synchronous) ------------------------------ */
+
+/* r[0..m+n) = a[0..m) * b[0..n), m, n >= 1.  Replaces mul_fpntt2!
+ * (src/fpntt.jl:982) and the NTT branch of mul!/mul_bal!
+ * (src/mul.jl:388-390, :161).  r must not alias a or b (fpntt.jl:979-981). */
+int nbg_mul(uint64_t *r, const uint64_t *a, int64_t m, const uint64_t *b, int64_t n);
+
+/* r[0..2n) = a[0..n)^2.  Replaces sqr_fpntt2! (src/fpntt.jl:1016) and the NTT
+ * branch of sqr! (src/mul.jl:141-147, :134). */
+int nbg_sqr(uint64_t *r, const uint64_t *a, int64_t n);
+
+/* ---- products, device buffers (asynchronous on `stream`, a cudaStream_t) - */
+
+int nbg_mul_dev(uint64_t *r, const uint64_t *a, int64_t m, const uint64_t *b, int64_t n, void *stream);
+int nbg_sqr_dev(uint64_t *r, const uint64_t *a, int64_t n, void *stream);
+
+/* ---- batches ------------------------------------------------------------- */
+
+/* One product of a batch.  b == NULL (or b == a with n == m) requests the
+ * square of a.  bits_a / bits_b are the operands' magnitude bits
+ * (64(n-1) + bit length of the top limb, kernels/addsub.jl:150); 0 asks the
+ * library to read the top limbs itself (one device-to-host copy for device
+ * batches). */
+typedef struct nbg_desc {
+    uint64_t *r;
+    const uint64_t *a;
+    const uint64_t *b;
+    int64_t m;
+    int64_t n;
+    int64_t bits_a;
+    int64_t bits_b;
+} nbg_desc;
+
+/* Whole batch in one call, host buffers, synchronous.  Products of any size
+ * run together in one launch per pipeline step. */
+int nbg_mul_batch(const nbg_desc *descs, int64_t count);
+
+/* Same with device buffers, asynchronous on `stream`. */
+int nbg_mul_batch_dev(const nbg_desc *descs, int64_t count, void *stream);
+
+/* Reusable batch over device buffers: plans, work queues and workspace are
+ * built once and the launch sequence is captured in a CUDA graph; each run
+ * replays it (operands may change between runs as long as their magnitude
+ * bits do not). */
+typedef struct nbg_batch nbg_batch;
+int nbg_batch_create(const nbg_desc *descs, int64_t count, nbg_batch **out);
+int nbg_batch_run(nbg_batch *bt, void *stream);
+/* number of kernel launches one nbg_batch_run issues */
+int nbg_batch_launches(const nbg_batch *bt);
+int nbg_batch_destroy(nbg_batch *bt);
+/* Per launch of a batch (up to cap): kernel kind (0 forward pass, 1 last pass
+ * with pointwise product, 2 reverse pass, 3 unpack, 4 carry), jobs, and the
+ * algorithmic FP64 instruction count and compulsory bytes of the reference
+ * schedule for that launch.  Any output pointer may be NULL. */
+int nbg_batch_stats(const nbg_batch *bt, int32_t *kinds, int64_t *njobs, double *alg_ops, double *alg_bytes,
+                    int32_t cap);
+/* Runs the batch's launches one by one (not as a graph) on `stream` with a
+ * CUDA event between launches; ms[i] = duration of launch i. */
+int nbg_batch_profile(nbg_batch *bt, void *stream, float *ms, int32_t cap);
+
+/* ---- admission (host-side restatement of the reference's sizing) -------- */
+
+/* fp_ntt_params (src/fpntt.jl:964-977): chunk width b and transform length N. */
+int nbg_ntt_params(int64_t bits_a, int64_t bits_b, int32_t *b, int64_t *N);
+/* ntt_len (src/fpntt.jl:936-951); NBG_ERANGE past 315*2^34. */
+int nbg_ntt_len(int64_t T, int64_t *N);
+/* magnitude_bits (src/kernels/addsub.jl:150) of a host operand. */
+int64_t nbg_magnitude_bits(const uint64_t *a, int64_t n);
+
+/* ---- transform-level entry points (device buffers; parity tests) --------- */
+
+/* fp_ntt_pack! (src/fpntt.jl:744-768): x[0..N) = b-bit chunks of limbs, zero filled. */
+int nbg_pack_dev(double *x, int64_t N, const uint64_t *limbs, int64_t n, int32_t b, int64_t nch, void *stream);
+/* fp_ntt_fwd! / fp_ntt_rev! (src/fpntt.jl:715-733) in place, prime 0 or 1. */
+int nbg_ntt_fwd_dev(double *x, int64_t N, int32_t prime, void *stream);
+int nbg_ntt_rev_dev(double *x, int64_t N, int32_t prime, void *stream);
+/* fp_ntt_pointwise! (src/fpntt.jl:770-785): xa[i] = mulmod(xa[i], xb[i]). */
+int nbg_pointwise_dev(double *xa, const double *xb, int64_t N, int32_t prime, void *stream);
+/* fp_ntt_unpack2! (src/fpntt.jl:869-925): r[0..rn) from the two reversed
+ * transforms of length N (both primes), nconv coefficients of b bits. */
+int nbg_unpack_dev(uint64_t *r, int64_t rn, const double *x1, const double *x2, int64_t N, int64_t nconv,
+                   int32_t b, void *stream);
+
+/* ---- plans and tuning ----------------------------------------------------- */
+
+/* Pass structure chosen for length N: fills up to `cap` entries of
+ * stage_m[] (radix per stage, forward order) and pass_end[] (last stage of each
+ * pass); returns via *nst, *npass. */
+int nbg_plan_info(int64_t N, int32_t *nst, int32_t *npass, int32_t *stage_m, int32_t *pass_end, int32_t cap);
+/* Host-only view of the plan for length N under the current tuning (no
+ * device needed): stages[3*i..] = (radix, span L, stride Q) in forward order,
+ * passes[6*j..] = (first stage, last stage, rows G, columns C, column stride
+ * Qb, tiles).  `cap` bounds both arrays' entry counts (stages and passes). */
+int nbg_plan_layout(int64_t N, int32_t sqr, int64_t *stages, int32_t *nst, int64_t *passes, int32_t *npass,
+                    int32_t cap);
+/* Tuning knobs (JSON object, keys: full_max_mul, full_max_sqr, last_max,
+ * early_gmax, tile_target, cmax).  Changing them drops cached plans. */
+int nbg_set_tuning(const char *json);
+/* Current tuning as a JSON object into buf (NUL-terminated). */
+int nbg_get_tuning(char *buf, int64_t cap);
+
+/* ---- device / errors ------------------------------------------------------ */
+
+int nbg_init(int32_t device);
+const char *nbg_last_error(void);
+/* the stream the synchronous host-buffer calls run on (a cudaStream_t) */
+void *nbg_default_stream(void);
+/* counters: kernel launches issued by this library since load */
+int64_t nbg_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NBGPU_H */

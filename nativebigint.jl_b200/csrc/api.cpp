@@ -1,0 +1,583 @@
+// api.cpp — the extern "C" entry points of include/nbgpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "../../include/nbgpu.h"
+#include "engine.h"
+#include "kernels.h"
+
+using namespace nbg;
+
+namespace {
+
+#define CUDA_TRY(x)                                                                         \
+    do {                                                                                    \
+        cudaError_t e_ = (x);                                                               \
+        if (e_ != cudaSuccess) return fail(NBG_ECUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+bool overlaps(const void* p, size_t pn, const void* q, size_t qn) {
+    const char* a = (const char*)p;
+    const char* b = (const char*)q;
+    return a < b + qn && b < a + pn;
+}
+
+// Validates one descriptor; fills a ProdIn (pointers left as given).
+int check_desc(const nbg_desc& d, ProdIn& q, bool host) {
+    if (!d.r || !d.a) return fail(NBG_EINVAL, "null pointer");
+    if (d.m < 1) return fail(NBG_EINVAL, "operand length %lld < 1", (long long)d.m);
+    const bool sqr = (d.b == nullptr) || (d.b == d.a && d.n == d.m);
+    if (!sqr && d.n < 1) return fail(NBG_EINVAL, "operand length %lld < 1", (long long)d.n);
+    const int64_t n = sqr ? d.m : d.n;
+    const size_t rb = sizeof(uint64_t) * (size_t)(d.m + n);
+    if (overlaps(d.r, rb, d.a, sizeof(uint64_t) * (size_t)d.m) ||
+        (!sqr && overlaps(d.r, rb, d.b, sizeof(uint64_t) * (size_t)n)))
+        return fail(NBG_EINVAL, "r must not alias a or b");
+    q.a = d.a;
+    q.b = sqr ? d.a : d.b;
+    q.r = d.r;
+    q.m = d.m;
+    q.n = n;
+    q.sqr = sqr ? 1 : 0;
+    q.bits_a = d.bits_a;
+    q.bits_b = sqr ? d.bits_a : d.bits_b;
+    if (host) {
+        q.bits_a = magnitude_bits(d.a, d.m);
+        q.bits_b = sqr ? q.bits_a : magnitude_bits(d.b, n);
+    }
+    return NBG_OK;
+}
+
+// pinned host staging for the host-buffer calls
+void* g_hpin = nullptr;
+size_t g_hpin_bytes = 0;
+int ensure_hpin(size_t bytes) {
+    if (bytes <= g_hpin_bytes) return NBG_OK;
+    if (g_hpin) cudaFreeHost(g_hpin);
+    g_hpin = nullptr;
+    g_hpin_bytes = 0;
+    size_t want = std::max(bytes, (size_t)16 << 20);
+    if (cudaHostAlloc(&g_hpin, want, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NBG_ENOMEM, "pinned staging of %zu bytes unavailable", want);
+    }
+    g_hpin_bytes = want;
+    return NBG_OK;
+}
+
+// Host-buffer batch: stage operands in pinned memory, one copy each way.
+int host_batch(const nbg_desc* descs, int64_t count) {
+    if (!descs || count <= 0) return fail(NBG_EINVAL, "empty batch");
+    Engine& E = g_eng;
+    std::vector<ProdIn> in((size_t)count);
+    for (int64_t k = 0; k < count; k++) {
+        int rc = check_desc(descs[k], in[(size_t)k], true);
+        if (rc) return rc;
+    }
+    {
+        int rc = E.ensure();
+        if (rc) return rc;
+    }
+    // operand/result layout in the staging area
+    std::vector<size_t> oa((size_t)count), ob((size_t)count), orr((size_t)count);
+    size_t ops = 0;
+    for (int64_t k = 0; k < count; k++) {
+        const ProdIn& q = in[(size_t)k];
+        oa[(size_t)k] = ops;
+        ops = align_up(ops + 8 * (size_t)q.m, 256);
+        if (!q.sqr) {
+            ob[(size_t)k] = ops;
+            ops = align_up(ops + 8 * (size_t)q.n, 256);
+        }
+    }
+    const size_t in_bytes = ops;
+    for (int64_t k = 0; k < count; k++) {
+        orr[(size_t)k] = ops;
+        ops = align_up(ops + 8 * (size_t)(in[(size_t)k].m + in[(size_t)k].n), 256);
+    }
+    const size_t out_bytes = ops - in_bytes;
+    BatchBuild bb;
+    int rc = build_batch(E, in.data(), count, bb);
+    if (rc) return rc;
+    const size_t dev_ops = align_up(bb.dev_bytes, 256);
+    rc = E.ensure_pool(dev_ops + ops);
+    if (rc) return rc;
+    rc = ensure_hpin(ops);
+    if (rc) return rc;
+    char* dbase = (char*)E.pool;
+    char* dop = dbase + dev_ops;
+    char* hp = (char*)g_hpin;
+    for (int64_t k = 0; k < count; k++) {
+        const ProdIn& q = in[(size_t)k];
+        memcpy(hp + oa[(size_t)k], q.a, 8 * (size_t)q.m);
+        if (!q.sqr) memcpy(hp + ob[(size_t)k], q.b, 8 * (size_t)q.n);
+        DProd& P = bb.prods[(size_t)k];
+        P.a = (const uint64_t*)(dop + oa[(size_t)k]);
+        P.b = q.sqr ? P.a : (const uint64_t*)(dop + ob[(size_t)k]);
+        P.r = (uint64_t*)(dop + orr[(size_t)k]);
+    }
+    cudaStream_t st = E.stream;
+    CUDA_TRY(cudaMemcpyAsync(dop, hp, in_bytes, cudaMemcpyHostToDevice, st));
+    rc = upload_batch(E, bb, dbase, st);
+    if (rc) return rc;
+    rc = run_launches(E, bb, dbase, st);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(hp + in_bytes, dop + in_bytes, out_bytes, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (int64_t k = 0; k < count; k++) {
+        const ProdIn& q = in[(size_t)k];
+        memcpy(q.r, hp + orr[(size_t)k], 8 * (size_t)(q.m + q.n));
+    }
+    return NBG_OK;
+}
+
+// Reads the operands' top limbs on the device (magnitude_bits) for
+// descriptors that leave bits_a / bits_b at 0.
+int fill_bits_dev(std::vector<ProdIn>& in, cudaStream_t st) {
+    std::vector<int64_t> need;
+    for (size_t k = 0; k < in.size(); k++)
+        if (in[k].bits_a <= 0 || (!in[k].sqr && in[k].bits_b <= 0)) need.push_back((int64_t)k);
+    if (need.empty()) return NBG_OK;
+    Engine& E = g_eng;
+    std::vector<DProd> tmp(need.size());
+    for (size_t i = 0; i < need.size(); i++) {
+        memset(&tmp[i], 0, sizeof(DProd));
+        const ProdIn& q = in[(size_t)need[i]];
+        tmp[i].a = q.a;
+        tmp[i].b = q.b;
+        tmp[i].m = q.m;
+        tmp[i].n = q.n;
+    }
+    const size_t pb = align_up(sizeof(DProd) * tmp.size(), 256);
+    const size_t bb = sizeof(int64_t) * 2 * tmp.size();
+    int rc = E.ensure_pool(pb + bb);
+    if (rc) return rc;
+    char* d = (char*)E.pool;
+    CUDA_TRY(cudaMemcpyAsync(d, tmp.data(), sizeof(DProd) * tmp.size(), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(launch_topbits((const DProd*)d, (int64_t)tmp.size(), (int64_t*)(d + pb), st));
+    g_launches++;
+    std::vector<int64_t> bits(2 * tmp.size());
+    CUDA_TRY(cudaMemcpyAsync(bits.data(), d + pb, bb, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < need.size(); i++) {
+        ProdIn& q = in[(size_t)need[i]];
+        q.bits_a = bits[2 * i];
+        q.bits_b = q.sqr ? q.bits_a : bits[2 * i + 1];
+    }
+    return NBG_OK;
+}
+
+int dev_batch(const nbg_desc* descs, int64_t count, cudaStream_t st) {
+    if (!descs || count <= 0) return fail(NBG_EINVAL, "empty batch");
+    Engine& E = g_eng;
+    std::vector<ProdIn> in((size_t)count);
+    for (int64_t k = 0; k < count; k++) {
+        int rc = check_desc(descs[k], in[(size_t)k], false);
+        if (rc) return rc;
+    }
+    int rc = E.ensure();
+    if (rc) return rc;
+    rc = fill_bits_dev(in, st);
+    if (rc) return rc;
+    BatchBuild bb;
+    rc = build_batch(E, in.data(), count, bb);
+    if (rc) return rc;
+    // the pool is reused by the next call: order it after earlier work on E.stream
+    rc = E.ensure_pool(bb.dev_bytes);
+    if (rc) return rc;
+    char* dbase = (char*)E.pool;
+    rc = upload_batch(E, bb, dbase, st);
+    if (rc) return rc;
+    rc = run_launches(E, bb, dbase, st);
+    if (rc) return rc;
+    // descriptors/jobs live in pageable host memory copied asynchronously;
+    // keep them valid until the copies ran.
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return NBG_OK;
+}
+
+cudaStream_t as_stream(void* s) { return s ? (cudaStream_t)s : g_eng.stream; }
+
+// One product descriptor wrapping a preloaded transform or an unpack.
+int transform_passes(double* x, int64_t N, int prime, bool fwd, cudaStream_t st) {
+    if (!x || prime < 0 || prime > 1) return fail(NBG_EINVAL, "bad argument");
+    Engine& E = g_eng;
+    PlanRec* pr;
+    int rc = E.get_plan(N, 0, &pr);
+    if (rc) return rc;
+    DProd P;
+    memset(&P, 0, sizeof P);
+    P.plan = pr->slot;
+    P.npass = pr->d.npass;
+    P.flags = PF_PRELOADED;
+    P.xa[prime] = x;
+    P.xa[1 - prime] = x;
+    std::vector<Job> jobs;
+    std::vector<Launch> ls;
+    const int np = pr->d.npass;
+    for (int i = 0; i < np; i++) {
+        const int p = fwd ? i : np - 1 - i;
+        const DPass& ps = pr->d.pass[p];
+        Launch L{fwd ? (int)JK_FWD : (int)JK_REV, (int64_t)jobs.size(), ps.ntiles,
+                 sizeof(double) * (size_t)ps.G * (size_t)ps.C};
+        for (int64_t t = 0; t < ps.ntiles; t++) jobs.push_back(Job{0, prime | (p << 8), t});
+        ls.push_back(L);
+    }
+    const size_t jo = 256;
+    rc = E.ensure_pool(jo + sizeof(Job) * jobs.size());
+    if (rc) return rc;
+    char* d = (char*)E.pool;
+    CUDA_TRY(cudaMemcpyAsync(d, &P, sizeof P, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(d + jo, jobs.data(), sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, st));
+    for (const Launch& L : ls) {
+        CUDA_TRY(launch_jobs(L.kind, (const DProd*)d, E.d_plans, (const Job*)(d + jo) + L.off, L.n, L.smem, 0, st));
+        g_launches++;
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return NBG_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+#define API_LOCK() std::lock_guard<std::recursive_mutex> lk_(g_eng.mu)
+#define API_LOCK_DEV()                                   \
+    std::lock_guard<std::recursive_mutex> lk_(g_eng.mu); \
+    {                                                    \
+        int rc_ = g_eng.ensure();                        \
+        if (rc_) return rc_;                             \
+    }
+
+extern "C" {
+
+int nbg_init(int32_t device) {
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    return g_eng.init(device);
+}
+
+const char* nbg_last_error(void) { return last_error(); }
+
+void* nbg_default_stream(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    if (g_eng.ensure()) return nullptr;
+    return (void*)g_eng.stream;
+}
+
+int64_t nbg_launch_count(void) { return g_launches.load(); }
+
+int nbg_mul(uint64_t* r, const uint64_t* a, int64_t m, const uint64_t* b, int64_t n) {
+    if (!b) return fail(NBG_EINVAL, "null pointer");
+    API_LOCK();
+    nbg_desc d{r, a, b, m, n, 0, 0};
+    return host_batch(&d, 1);
+}
+
+int nbg_sqr(uint64_t* r, const uint64_t* a, int64_t n) {
+    API_LOCK();
+    nbg_desc d{r, a, nullptr, n, n, 0, 0};
+    return host_batch(&d, 1);
+}
+
+int nbg_mul_dev(uint64_t* r, const uint64_t* a, int64_t m, const uint64_t* b, int64_t n, void* stream) {
+    if (!b) return fail(NBG_EINVAL, "null pointer");
+    API_LOCK();
+    nbg_desc d{r, a, b, m, n, 0, 0};
+    return dev_batch(&d, 1, as_stream(stream));
+}
+
+int nbg_sqr_dev(uint64_t* r, const uint64_t* a, int64_t n, void* stream) {
+    API_LOCK();
+    nbg_desc d{r, a, nullptr, n, n, 0, 0};
+    return dev_batch(&d, 1, as_stream(stream));
+}
+
+int nbg_mul_batch(const nbg_desc* descs, int64_t count) {
+    API_LOCK();
+    return host_batch(descs, count);
+}
+
+int nbg_mul_batch_dev(const nbg_desc* descs, int64_t count, void* stream) {
+    API_LOCK();
+    return dev_batch(descs, count, as_stream(stream));
+}
+
+// ---- reusable batches (CUDA graph) ----------------------------------------
+
+struct nbg_batch {
+    BatchBuild bb;
+    char* dmem = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+int nbg_batch_create(const nbg_desc* descs, int64_t count, nbg_batch** out) {
+    if (!out) return fail(NBG_EINVAL, "null out");
+    API_LOCK();
+    *out = nullptr;
+    if (!descs || count <= 0) return fail(NBG_EINVAL, "empty batch");
+    Engine& E = g_eng;
+    std::vector<ProdIn> in((size_t)count);
+    for (int64_t k = 0; k < count; k++) {
+        int rc = check_desc(descs[k], in[(size_t)k], false);
+        if (rc) return rc;
+    }
+    int rc = E.ensure();
+    if (rc) return rc;
+    rc = fill_bits_dev(in, E.stream);
+    if (rc) return rc;
+    nbg_batch* bt = new nbg_batch();
+    rc = build_batch(E, in.data(), count, bt->bb);
+    if (rc) {
+        delete bt;
+        return rc;
+    }
+    if (cudaMalloc(&bt->dmem, bt->bb.dev_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        const size_t want = bt->bb.dev_bytes;
+        delete bt;
+        return fail(NBG_ENOMEM, "batch workspace of %zu bytes unavailable", want);
+    }
+    rc = upload_batch(E, bt->bb, bt->dmem, E.stream);
+    if (!rc && cudaStreamSynchronize(E.stream) != cudaSuccess) rc = fail(NBG_ECUDA, "batch upload failed");
+    if (!rc) {
+        cudaStream_t cs;
+        if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+            rc = fail(NBG_ECUDA, "stream create failed");
+        } else {
+            if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                rc = fail(NBG_ECUDA, "begin capture failed");
+            } else {
+                int64_t before = g_launches.load();
+                int rl = run_launches(E, bt->bb, bt->dmem, cs);
+                g_launches.store(before);  // captured, not issued
+                cudaError_t ec = cudaStreamEndCapture(cs, &bt->graph);
+                if (rl) rc = rl;
+                else if (ec != cudaSuccess) rc = fail(NBG_ECUDA, "end capture: %s", cudaGetErrorString(ec));
+                else if (cudaGraphInstantiate(&bt->exec, bt->graph, 0) != cudaSuccess)
+                    rc = fail(NBG_ECUDA, "graph instantiate failed");
+            }
+            cudaStreamDestroy(cs);
+        }
+    }
+    if (rc) {
+        if (bt->exec) cudaGraphExecDestroy(bt->exec);
+        if (bt->graph) cudaGraphDestroy(bt->graph);
+        cudaFree(bt->dmem);
+        delete bt;
+        return rc;
+    }
+    *out = bt;
+    return NBG_OK;
+}
+
+int nbg_batch_run(nbg_batch* bt, void* stream) {
+    if (!bt) return fail(NBG_EINVAL, "null batch");
+    API_LOCK_DEV();
+    CUDA_TRY(cudaGraphLaunch(bt->exec, as_stream(stream)));
+    g_launches += (int64_t)bt->bb.launches.size();
+    return NBG_OK;
+}
+
+int nbg_batch_launches(const nbg_batch* bt) { return bt ? (int)bt->bb.launches.size() : 0; }
+
+int nbg_batch_stats(const nbg_batch* bt, int32_t* kinds, int64_t* njobs, double* alg_ops, double* alg_bytes,
+                    int32_t cap) {
+    if (!bt || cap < 0) return fail(NBG_EINVAL, "bad argument");
+    const auto& ls = bt->bb.launches;
+    for (size_t i = 0; i < ls.size() && (int32_t)i < cap; i++) {
+        if (kinds) kinds[i] = ls[i].kind;
+        if (njobs) njobs[i] = ls[i].n;
+        if (alg_ops) alg_ops[i] = ls[i].alg_ops;
+        if (alg_bytes) alg_bytes[i] = ls[i].alg_bytes;
+    }
+    return NBG_OK;
+}
+
+int nbg_batch_profile(nbg_batch* bt, void* stream, float* ms, int32_t cap) {
+    if (!bt || !ms) return fail(NBG_EINVAL, "bad argument");
+    API_LOCK_DEV();
+    cudaStream_t st = as_stream(stream);
+    const auto& ls = bt->bb.launches;
+    std::vector<cudaEvent_t> ev(ls.size() + 1);
+    for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+    const DProd* prods = (const DProd*)(bt->dmem + bt->bb.off_prods);
+    const Job* jobs = (const Job*)(bt->dmem + bt->bb.off_jobs);
+    int rc = NBG_OK;
+    CUDA_TRY(cudaEventRecord(ev[0], st));
+    for (size_t i = 0; i < ls.size(); i++) {
+        const Launch& L = ls[i];
+        cudaError_t e = launch_jobs(L.kind, prods, g_eng.d_plans, jobs + L.off, L.n, L.smem, 0, st);
+        if (e != cudaSuccess) { rc = fail(NBG_ECUDA, "profile launch: %s", cudaGetErrorString(e)); break; }
+        g_launches++;
+        CUDA_TRY(cudaEventRecord(ev[i + 1], st));
+    }
+    if (!rc && cudaEventSynchronize(ev[ls.size()]) != cudaSuccess) rc = fail(NBG_ECUDA, "profile sync failed");
+    for (size_t i = 0; !rc && i < ls.size() && (int32_t)i < cap; i++) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+int nbg_batch_destroy(nbg_batch* bt) {
+    if (!bt) return NBG_OK;
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    if (bt->exec) cudaGraphExecDestroy(bt->exec);
+    if (bt->graph) cudaGraphDestroy(bt->graph);
+    if (bt->dmem) cudaFree(bt->dmem);
+    delete bt;
+    return NBG_OK;
+}
+
+// ---- admission -------------------------------------------------------------
+
+int nbg_ntt_params(int64_t bits_a, int64_t bits_b, int32_t* b, int64_t* N) {
+    if (!b || !N || bits_a < 1 || bits_b < 1) return fail(NBG_EINVAL, "bad argument");
+    int bb;
+    int rc = ntt_params(bits_a, bits_b, &bb, N);
+    if (rc) return rc;
+    *b = bb;
+    return NBG_OK;
+}
+
+int nbg_ntt_len(int64_t T, int64_t* N) {
+    if (!N || T < 1) return fail(NBG_EINVAL, "bad argument");
+    int64_t v = ntt_len(T);
+    if (v < 0) return fail(NBG_ERANGE, "fp NTT length %lld exceeds the 315*2^34 the primes support", (long long)T);
+    *N = v;
+    return NBG_OK;
+}
+
+int64_t nbg_magnitude_bits(const uint64_t* a, int64_t n) {
+    if (!a || n < 1) return -1;
+    return magnitude_bits(a, n);
+}
+
+// ---- transform level --------------------------------------------------------
+
+int nbg_pack_dev(double* x, int64_t N, const uint64_t* limbs, int64_t n, int32_t b, int64_t nch, void* stream) {
+    if (!x || !limbs || n < 1 || b < 1 || b > 52 || nch < 0 || nch > N) return fail(NBG_EINVAL, "bad argument");
+    if ((nch - 1) * (int64_t)b >= 64 * n) return fail(NBG_EINVAL, "nch exceeds the operand");
+    API_LOCK_DEV();
+    CUDA_TRY(launch_pack(x, N, limbs, n, b, nch, as_stream(stream)));
+    g_launches++;
+    return NBG_OK;
+}
+
+int nbg_ntt_fwd_dev(double* x, int64_t N, int32_t prime, void* stream) {
+    API_LOCK_DEV();
+    return transform_passes(x, N, prime, true, as_stream(stream));
+}
+
+int nbg_ntt_rev_dev(double* x, int64_t N, int32_t prime, void* stream) {
+    API_LOCK_DEV();
+    return transform_passes(x, N, prime, false, as_stream(stream));
+}
+
+int nbg_pointwise_dev(double* xa, const double* xb, int64_t N, int32_t prime, void* stream) {
+    if (!xa || !xb || N < 1 || prime < 0 || prime > 1) return fail(NBG_EINVAL, "bad argument");
+    API_LOCK_DEV();
+    CUDA_TRY(launch_pointwise(xa, xb, N, prime, as_stream(stream)));
+    g_launches++;
+    return NBG_OK;
+}
+
+int nbg_unpack_dev(uint64_t* r, int64_t rn, const double* x1, const double* x2, int64_t N, int64_t nconv, int32_t b,
+                   void* stream) {
+    if (!r || !x1 || !x2 || rn < 1 || nconv < 1 || nconv > N || b < 1 || b > 52) return fail(NBG_EINVAL, "bad argument");
+    API_LOCK_DEV();
+    Engine& E = g_eng;
+    cudaStream_t st = as_stream(stream);
+    PlanRec* pr;
+    int rc = E.get_plan(N, 0, &pr);
+    if (rc) return rc;
+    DProd P;
+    memset(&P, 0, sizeof P);
+    P.plan = pr->slot;
+    P.r = r;
+    P.rn = rn;
+    P.nconv = nconv;
+    P.bch = b;
+    P.xa[0] = (double*)x1;
+    P.xa[1] = (double*)x2;
+    P.ntl = (rn + UNPACK_TL - 1) / UNPACK_TL;
+    std::vector<Job> jobs;
+    for (int64_t t = 0; t < P.ntl; t++) jobs.push_back(Job{0, 0, t});
+    jobs.push_back(Job{0, 0, 0});
+    const size_t jo = 256, ao = align_up(jo + sizeof(Job) * jobs.size(), 256);
+    rc = E.ensure_pool(ao + sizeof(uint32_t) * (size_t)P.ntl);
+    if (rc) return rc;
+    char* d = (char*)E.pool;
+    P.agg = (uint32_t*)(d + ao);
+    CUDA_TRY(cudaMemcpyAsync(d, &P, sizeof P, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(d + jo, jobs.data(), sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, st));
+    const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / b + 4;
+    CUDA_TRY(launch_jobs(JK_UNPACK, (const DProd*)d, E.d_plans, (const Job*)(d + jo), P.ntl,
+                         sizeof(uint64_t) * 2 * align_up((size_t)ncoef, 2), 0, st));
+    CUDA_TRY(launch_jobs(JK_CARRY, (const DProd*)d, E.d_plans, (const Job*)(d + jo) + P.ntl, 1, 0, 0, st));
+    g_launches += 2;
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return NBG_OK;
+}
+
+// ---- plans / tuning ---------------------------------------------------------
+
+int nbg_plan_info(int64_t N, int32_t* nst, int32_t* npass, int32_t* stage_m, int32_t* pass_end, int32_t cap) {
+    if (!nst || !npass) return fail(NBG_EINVAL, "bad argument");
+    API_LOCK_DEV();
+    PlanRec* pr;
+    int rc = g_eng.get_plan(N, 0, &pr);
+    if (rc) return rc;
+    *nst = pr->d.nst;
+    *npass = pr->d.npass;
+    for (int i = 0; stage_m && i < pr->d.nst && i < cap; i++) stage_m[i] = pr->d.st[i].m;
+    for (int i = 0; pass_end && i < pr->d.npass && i < cap; i++) pass_end[i] = pr->d.pass[i].sb;
+    return NBG_OK;
+}
+
+int nbg_plan_layout(int64_t N, int32_t sqr, int64_t* stages, int32_t* nst, int64_t* passes, int32_t* npass,
+                    int32_t cap) {
+    if (!stages || !nst || !passes || !npass || cap < 1) return fail(NBG_EINVAL, "bad argument");
+    API_LOCK();
+    DPlan d;
+    int rc = plan_structure(N, sqr, g_eng.tun, d);
+    if (rc) return rc;
+    if (d.nst > cap || d.npass > cap) return fail(NBG_EINVAL, "cap too small");
+    for (int i = 0; i < d.nst; i++) {
+        stages[3 * i] = d.st[i].m;
+        stages[3 * i + 1] = d.st[i].L;
+        stages[3 * i + 2] = d.st[i].Q;
+    }
+    for (int j = 0; j < d.npass; j++) {
+        const DPass& p = d.pass[j];
+        int64_t* o = passes + 6 * j;
+        o[0] = p.sa; o[1] = p.sb; o[2] = p.G; o[3] = p.C; o[4] = p.Qb; o[5] = p.ntiles;
+    }
+    *nst = d.nst;
+    *npass = d.npass;
+    return NBG_OK;
+}
+
+int nbg_set_tuning(const char* json) {
+    if (!json) return fail(NBG_EINVAL, "null json");
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    int rc = g_eng.tun.from_json(json);
+    if (rc) return rc;
+    g_eng.drop_plans();
+    return NBG_OK;
+}
+
+int nbg_get_tuning(char* buf, int64_t cap) {
+    if (!buf || cap < 2) return fail(NBG_EINVAL, "bad argument");
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    std::string s = g_eng.tun.to_json();
+    if ((int64_t)s.size() + 1 > cap) return fail(NBG_EINVAL, "buffer too small");
+    memcpy(buf, s.c_str(), s.size() + 1);
+    return NBG_OK;
+}
+
+}  // extern "C"

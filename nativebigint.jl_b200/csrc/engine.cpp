@@ -1,0 +1,709 @@
+// engine.cpp — host side of libnbgpu.so: admission, plans, batch work queues
+// and the C ABI declared in include/nbgpu.h.
+//
+// Host restatements (all exact, same results as the reference):
+//   magnitude_bits      src/kernels/addsub.jl:150
+//   ntt_len             src/fpntt.jl:927-951
+//   fp_ntt_params       src/fpntt.jl:953-977
+//   plan / constants    src/fpntt.jl:50-79 (primes, generator), :123-168
+//                       (Winograd constants), :191-271 (stage list)
+// This file is compiled with -ffp-contract=off so the double arithmetic that
+// builds the combine constants matches the reference's bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/nbgpu.h"
+#include "engine.h"
+#include "consts.h"
+#include "kernels.h"
+
+namespace nbg {
+
+// ---------------------------------------------------------------------------
+// errors
+
+static thread_local std::string t_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_err = buf;
+    return code;
+}
+const char* last_error() { return t_err.c_str(); }
+
+#define CUDA_TRY(x)                                                                         \
+    do {                                                                                    \
+        cudaError_t e_ = (x);                                                               \
+        if (e_ != cudaSuccess) return fail(NBG_ECUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)
+
+std::atomic<int64_t> g_launches{0};
+
+// ---------------------------------------------------------------------------
+// exact host arithmetic
+
+typedef unsigned __int128 u128;
+static inline uint64_t mulmod_u(uint64_t a, uint64_t b, uint64_t p) { return (uint64_t)(((u128)a * b) % p); }
+static uint64_t powmod_u(uint64_t a, uint64_t e, uint64_t p) {
+    uint64_t r = 1 % p;
+    a %= p;
+    while (e) {
+        if (e & 1) r = mulmod_u(r, a, p);
+        a = mulmod_u(a, a, p);
+        e >>= 1;
+    }
+    return r;
+}
+static uint64_t invmod_u(uint64_t a, uint64_t p) { return powmod_u(a, p - 2, p); }
+
+static const uint64_t PR[2] = {P1_U, P2_U};
+static const int TWOADIC[2] = {34, 38};
+static const uint64_t FACS[2][5] = {{2, 3, 5, 7, 23}, {2, 3, 5, 7, 13}};
+
+// fp_generator (fpntt.jl:50-56)
+static uint64_t generator(int f) {
+    static uint64_t g[2] = {0, 0};
+    if (!g[f]) {
+        uint64_t p = PR[f];
+        for (uint64_t c = 3; c <= 63; c++) {
+            bool ok = true;
+            for (int i = 0; i < 5; i++)
+                if (powmod_u(c, (p - 1) / FACS[f][i], p) == 1) ok = false;
+            if (ok) { g[f] = c; break; }
+        }
+    }
+    return g[f];
+}
+
+// host field ops (fpntt.jl:81-121)
+static inline double h_round(double v) { return (v + FP_MAGIC) - FP_MAGIC; }
+static inline double h_reduce(double x, double P) {
+    double q = h_round(x * (1.0 / P));
+    return std::fma(q, -P, x);
+}
+static inline double h_mulmod(double x, double y, double P) {
+    double h = x * y;
+    double l = std::fma(x, y, -h);
+    return h_reduce(h, P) + l;
+}
+static inline double h_minbal(double x, double P) { return x > P / 2 ? x - P : (x < -P / 2 ? x + P : x); }
+
+// fp_dft5_consts (fpntt.jl:127-136)
+static void dft5_consts(uint64_t c, double P, uint64_t p, double* out) {
+    double inv2 = (double)invmod_u(2, p);
+    double c1 = h_reduce((double)c, P);
+    double c2 = h_mulmod(c1, c1, P), c3 = h_mulmod(c2, c1, P), c4 = h_mulmod(c3, c1, P);
+    double inv4 = h_mulmod(inv2, inv2, P);
+    out[0] = h_minbal(-inv4, P);
+    out[1] = h_minbal(h_mulmod((c1 + c4) - (c2 + c3), inv4, P), P);
+    out[2] = h_minbal(h_mulmod(c1 - c4, inv2, P), P);
+    out[3] = h_minbal(h_mulmod(c2 - c3, inv2, P), P);
+}
+
+// fp_dft7_consts (fpntt.jl:151-168)
+static void dft7_consts(uint64_t c, double P, uint64_t p, double* out) {
+    double inv2 = (double)invmod_u(2, p), inv3 = (double)invmod_u(3, p);
+    double cj[7];
+    for (int j = 1; j <= 6; j++) cj[j] = (double)powmod_u(c, (uint64_t)j, p);
+    auto A = [&](int j) { return h_mulmod(cj[j] + cj[7 - j], inv2, P); };
+    auto B = [&](int j) { return h_mulmod(cj[j] - cj[7 - j], inv2, P); };
+    double a0 = A(1), a1 = A(3), a2 = A(2);
+    double b0 = B(1), b1 = B(3), b2 = B(2);
+    double bp0 = h_minbal(h_mulmod(a0 - a2, inv3, P), P);
+    double bp1 = h_minbal(h_mulmod(a1 - a2, inv3, P), P);
+    double n0 = h_minbal(h_mulmod(b0 - b2, inv3, P), P);
+    double n1 = h_minbal(h_mulmod(b1 + b2, inv3, P), P);
+    out[0] = h_minbal(h_mulmod((a0 + a1) + a2, inv3, P), P);
+    out[1] = bp0;
+    out[2] = bp1;
+    out[3] = h_minbal(bp0 + bp1, P);
+    out[4] = h_minbal(h_mulmod((b0 + b2) - b1, inv3, P), P);
+    out[5] = n0;
+    out[6] = n1;
+    out[7] = h_minbal(n0 + n1, P);
+}
+
+// ---------------------------------------------------------------------------
+// admission
+
+static inline int tsb64(uint64_t x) { return x ? 64 - __builtin_clzll(x) : 0; }
+static inline int tsb128(u128 x) {
+    uint64_t hi = (uint64_t)(x >> 64);
+    return hi ? 64 + tsb64(hi) : tsb64((uint64_t)x);
+}
+
+int64_t magnitude_bits(const uint64_t* a, int64_t n) { return 64 * (n - 1) + tsb64(a[n - 1]); }
+
+int64_t ntt_len(int64_t T) {
+    static const int64_t SMALL[] = {1, 3, 5, 9}, MID[] = {1, 3, 5, 7, 9, 15, 21, 105},
+                         LARGE[] = {1, 3, 5, 7, 9, 15, 21, 35, 45, 63, 105, 315};
+    const int maxk = std::min(TWOADIC[0], TWOADIC[1]);
+    const int64_t* ms;
+    int nm;
+    if (T <= (int64_t(1) << 14)) { ms = SMALL; nm = 4; }
+    else if (T <= (int64_t(1) << 20)) { ms = MID; nm = 8; }
+    else { ms = LARGE; nm = 12; }
+    int64_t best = INT64_MAX;
+    for (int i = 0; i < nm; i++) {
+        int64_t m = ms[i];
+        int64_t cl = (T + m - 1) / m;
+        int k = std::max(tsb64((uint64_t)(cl - 1)), 2);
+        if (k > maxk) continue;
+        best = std::min(best, m << k);
+    }
+    return best == INT64_MAX ? -1 : best;
+}
+
+int ntt_params(int64_t bits_a, int64_t bits_b, int* b_out, int64_t* N_out) {
+    const u128 pp = (u128)PR[0] * PR[1] - 1;
+    const int maxb = tsb64(std::min(PR[0], PR[1])) - 1;
+    const int64_t mn = std::min(bits_a, bits_b);
+    const int nclow = tsb64((uint64_t)((mn + maxb - 1) / maxb));
+    const int bstart = std::min(maxb, (tsb128(pp) - nclow + 3) >> 1);
+    for (int b = bstart; b >= 1; b--) {
+        int64_t nca = (bits_a + b - 1) / b, ncb = (bits_b + b - 1) / b;
+        u128 w = (u128)((1ULL << b) - 1);
+        if ((u128)std::min(nca, ncb) <= pp / (w * w)) {
+            int64_t N = ntt_len(nca + ncb - 1);
+            if (N < 0) return fail(NBG_ERANGE, "fp NTT length %lld exceeds the 315*2^34 the primes support",
+                                   (long long)(nca + ncb - 1));
+            *b_out = b;
+            *N_out = N;
+            return NBG_OK;
+        }
+    }
+    return fail(NBG_ERANGE, "no admissible chunk width");
+}
+
+// ---------------------------------------------------------------------------
+// tuning
+
+static int64_t pow2floor(int64_t x) {
+    int64_t r = 1;
+    while (r * 2 <= x) r *= 2;
+    return r;
+}
+
+std::string Tuning::to_json() const {
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "{\"full_max_mul\": %d, \"full_max_sqr\": %d, \"last_max\": %d, \"early_gmax\": %d, "
+             "\"tile_target\": %d, \"cmax\": %d}",
+             full_max_mul, full_max_sqr, last_max, early_gmax, tile_target, cmax);
+    return buf;
+}
+
+static bool json_int(const char* js, const char* key, int* out) {
+    std::string k = std::string("\"") + key + "\"";
+    const char* p = strstr(js, k.c_str());
+    if (!p) return false;
+    p = strchr(p + k.size(), ':');
+    if (!p) return false;
+    char* end = nullptr;
+    long v = strtol(p + 1, &end, 10);
+    if (end == p + 1) return false;
+    *out = (int)v;
+    return true;
+}
+
+int Tuning::from_json(const char* js) {
+    Tuning t = *this;
+    json_int(js, "full_max_mul", &t.full_max_mul);
+    json_int(js, "full_max_sqr", &t.full_max_sqr);
+    json_int(js, "last_max", &t.last_max);
+    json_int(js, "early_gmax", &t.early_gmax);
+    json_int(js, "tile_target", &t.tile_target);
+    json_int(js, "cmax", &t.cmax);
+    auto pow2 = [](int v) { return v >= 1 && (v & (v - 1)) == 0; };
+    if (!pow2(t.cmax) || t.last_max < 4 || t.early_gmax < 2 || t.tile_target < 1 || t.full_max_mul < 4 ||
+        t.full_max_sqr < 4 || t.full_max_mul > 8192 || t.full_max_sqr > 16384 || t.last_max > 8192 ||
+        t.early_gmax > 4096 || t.tile_target > 8192)
+        return fail(NBG_EINVAL, "tuning out of range");
+    *this = t;
+    return NBG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// engine
+
+Engine g_eng;
+
+int Engine::init(int device) {
+    if (ready) {
+        if (device != dev) return fail(NBG_EINVAL, "engine already bound to device %d", dev);
+        return NBG_OK;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(NBG_ENODEV, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(NBG_EINVAL, "device %d out of range", device);
+    CUDA_TRY(cudaSetDevice(device));
+    CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CUDA_TRY(kernels_init((double)PR[0], (double)PR[1]));
+    CUDA_TRY(cudaMalloc(&d_plans, sizeof(DPlan) * (size_t)plan_cap));
+    CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    smem_optin = kernels_smem_optin();
+    dev = device;
+    ready = true;
+    return NBG_OK;
+}
+
+int Engine::ensure() {
+    if (ready) {
+        cudaSetDevice(dev);
+        return NBG_OK;
+    }
+    return init(0);
+}
+
+// Stage list, combine constants and pass split for length N (build_fp_plan,
+// fpntt.jl:236-271).  Host only; the twiddle tables are added by build_plan.
+int plan_structure(int64_t N, int for_sqr, const Tuning& tun, DPlan& d) {
+    if (N < 4) return fail(NBG_EINVAL, "transform length %lld < 4", (long long)N);
+    const int k = __builtin_ctzll((uint64_t)N);
+    const int64_t m = N >> k;
+    static const int64_t okm[] = {1, 3, 5, 7, 9, 15, 21, 35, 45, 63, 105, 315};
+    bool okm_hit = false;
+    for (int64_t v : okm) okm_hit |= (m == v);
+    if (!okm_hit || !(m == 1 || k >= 2) || k > std::min(TWOADIC[0], TWOADIC[1]))
+        return fail(NBG_EINVAL, "inadmissible transform length %lld", (long long)N);
+    if (N > (int64_t(1) << 33)) return fail(NBG_ENOMEM, "transform length %lld too large for one GPU", (long long)N);
+
+    memset(&d, 0, sizeof d);
+    d.N = N;
+    struct HS { int m; int64_t L, Q; };
+    std::vector<HS> hs;
+    int64_t span = N, mm = m;
+    for (int mf : {7, 5, 3, 3})
+        if (mm % mf == 0) {
+            hs.push_back({mf, span, span / mf});
+            span /= mf;
+            mm /= mf;
+        }
+    const int64_t N2 = span;
+    for (int64_t L = N2; L >= 4; L >>= 2) hs.push_back({4, L, L / 4});
+    if (__builtin_ctzll((uint64_t)N2) & 1) hs.push_back({2, 2, 1});
+    const int S = (int)hs.size();
+    if (S > MAXST) return fail(NBG_EINVAL, "too many stages");
+    d.nst = S;
+    for (int s = 0; s < S; s++) {
+        d.st[s].m = hs[s].m;
+        d.st[s].L = hs[s].L;
+        d.st[s].Q = hs[s].Q;
+    }
+
+    // combine constants per prime
+    for (int f = 0; f < 2; f++) {
+        const uint64_t p = PR[f];
+        const double P = (double)p;
+        uint64_t r = powmod_u(generator(f), (p - 1) / (uint64_t)N, p);
+        int s = 0;
+        for (; s < S && hs[s].m != 4 && hs[s].m != 2; s++) {
+            uint64_t c = powmod_u(r, (uint64_t)hs[s].Q, p);
+            double* rot = d.st[s].rot[f];
+            if (hs[s].m == 5) dft5_consts(c, P, p, rot);
+            else if (hs[s].m == 7) dft7_consts(c, P, p, rot);
+            else
+                for (int t = 1; t < hs[s].m; t++) rot[t - 1] = h_reduce((double)powmod_u(c, (uint64_t)t, p), P);
+            r = powmod_u(r, (uint64_t)hs[s].m, p);
+        }
+        double wi = N2 >= 4 ? h_reduce((double)powmod_u(r, (uint64_t)(N2 >> 2), p), P) : 1.0;
+        for (; s < S; s++) d.st[s].rot[f][0] = (hs[s].m == 4) ? wi : 0.0;
+        d.ninv[f] = h_reduce((double)invmod_u((uint64_t)N % p, p), P);
+        d.ninvp[f] = d.ninv[f] / P;
+    }
+
+    // pass split: the last pass is the longest suffix whose span fits
+    // last_max (a contiguous block, C = 1); earlier stages are grouped
+    // greedily into column passes of at most early_gmax rows.
+    const int full_max = for_sqr ? tun.full_max_sqr : tun.full_max_mul;
+    int a = 0;
+    if (N > full_max) {
+        a = S - 1;
+        for (int s = 0; s < S; s++)
+            if (hs[s].L <= tun.last_max) { a = s; break; }
+        if (a == 0) a = 1;
+    }
+    int np = 0;
+    int sa = 0;
+    while (sa < a) {
+        int sb = sa;
+        while (sb + 1 < a && hs[sa].L / hs[sb + 1].Q <= tun.early_gmax) sb++;
+        const int64_t Qb = hs[sb].Q;
+        const int64_t G = hs[sa].L / Qb;
+        const int64_t low = Qb & -Qb;
+        int64_t C = std::min<int64_t>(low, std::min<int64_t>(tun.cmax, pow2floor(std::max<int64_t>(1, tun.tile_target / G))));
+        if (np >= MAXPASS - 1) return fail(NBG_EINVAL, "too many passes for N=%lld", (long long)N);
+        DPass& ps = d.pass[np++];
+        ps.sa = sa;
+        ps.sb = sb;
+        ps.G = (int32_t)G;
+        ps.C = (int32_t)C;
+        ps.Qb = Qb;
+        ps.ntiles = (N / hs[sa].L) * (Qb / C);
+        sa = sb + 1;
+    }
+    {
+        DPass& ps = d.pass[np++];
+        ps.sa = a;
+        ps.sb = S - 1;
+        ps.G = (int32_t)hs[a].L;
+        ps.C = 1;
+        ps.Qb = 1;
+        ps.ntiles = N / hs[a].L;
+    }
+    d.npass = np;
+    return NBG_OK;
+}
+
+// Plan with device twiddle tables (one allocation for both primes).
+int Engine::build_plan(int64_t N, PlanRec& pr, int for_sqr) {
+    DPlan& d = pr.d;
+    int prc = plan_structure(N, for_sqr, tun, d);
+    if (prc) return prc;
+    const int S = d.nst;
+    struct HS { int m; int64_t L, Q; };
+    std::vector<HS> hs((size_t)S);
+    for (int s = 0; s < S; s++) hs[(size_t)s] = {d.st[s].m, d.st[s].L, d.st[s].Q};
+
+    // twiddle tables: per prime sum_s (m_s - 1) Q_s doubles, expanded on device
+    size_t per = 0;
+    for (int s = 0; s < S; s++)
+        if (hs[s].m != 2) per += (size_t)(hs[s].m - 1) * (size_t)hs[s].Q;
+    const int64_t nhi = (N + 4095) / 4096;
+    std::vector<double> hilo((size_t)(nhi + 4096));
+    double* dtab = nullptr;
+    double* dtmp = nullptr;
+    CUDA_TRY(cudaMalloc(&dtab, sizeof(double) * 2 * per));
+    if (cudaMalloc(&dtmp, sizeof(double) * hilo.size()) != cudaSuccess) {
+        cudaFree(dtab);
+        return fail(NBG_ENOMEM, "twiddle staging allocation failed");
+    }
+    int rc = NBG_OK;
+    for (int f = 0; f < 2 && rc == NBG_OK; f++) {
+        const uint64_t p = PR[f];
+        const double P = (double)p;
+        const uint64_t w = powmod_u(generator(f), (p - 1) / (uint64_t)N, p);
+        const uint64_t w4096 = powmod_u(w, 4096, p);
+        uint64_t x = 1;
+        for (int64_t i = 0; i < nhi; i++) {
+            hilo[(size_t)i] = h_minbal((double)x, P);
+            x = mulmod_u(x, w4096, p);
+        }
+        x = 1;
+        for (int i = 0; i < 4096; i++) {
+            hilo[(size_t)(nhi + i)] = h_minbal((double)x, P);
+            x = mulmod_u(x, w, p);
+        }
+        if (cudaMemcpyAsync(dtmp, hilo.data(), sizeof(double) * hilo.size(), cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess) {
+            rc = fail(NBG_ECUDA, "twiddle upload failed");
+            break;
+        }
+        size_t off = (size_t)f * per;
+        for (int s = 0; s < S; s++) {
+            if (hs[s].m == 2) {
+                d.st[s].tw[f] = nullptr;
+                continue;
+            }
+            double* out = dtab + off;
+            d.st[s].tw[f] = out;
+            if (launch_twiddle(out, hs[s].m, hs[s].Q, N / hs[s].L, dtmp, dtmp + nhi, f, stream) != cudaSuccess) {
+                rc = fail(NBG_ECUDA, "twiddle kernel launch failed");
+                break;
+            }
+            g_launches++;
+            off += (size_t)(hs[s].m - 1) * (size_t)hs[s].Q;
+        }
+        // hilo is reused for the second prime: wait for the copy to finish
+        if (cudaStreamSynchronize(stream) != cudaSuccess) rc = fail(NBG_ECUDA, "twiddle build failed");
+    }
+    cudaFree(dtmp);
+    if (rc != NBG_OK) {
+        cudaFree(dtab);
+        return rc;
+    }
+    pr.dtab = dtab;
+    pr.table_bytes = sizeof(double) * 2 * per;
+    if (plan_used >= plan_cap) return fail(NBG_ENOMEM, "plan slots exhausted");
+    pr.slot = plan_used++;
+    CUDA_TRY(cudaMemcpyAsync(d_plans + pr.slot, &d, sizeof(DPlan), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    return NBG_OK;
+}
+
+int Engine::get_plan(int64_t N, int for_sqr, PlanRec** out) {
+    const int64_t key = N * 2 + (for_sqr ? 1 : 0);
+    auto it = plans.find(key);
+    if (it != plans.end()) {
+        *out = &it->second;
+        return NBG_OK;
+    }
+    PlanRec pr;
+    int rc = build_plan(N, pr, for_sqr);
+    if (rc) return rc;
+    auto ins = plans.emplace(key, pr);
+    *out = &ins.first->second;
+    return NBG_OK;
+}
+
+void Engine::drop_plans() {
+    // Tables of dropped plans stay allocated: graphs of live batches may still
+    // reference them.  Only the lookup is reset.
+    for (auto& kv : plans) graveyard.push_back(kv.second.dtab);
+    plans.clear();
+}
+
+int Engine::ensure_pool(size_t bytes) {
+    if (bytes <= pool_bytes) return NBG_OK;
+    if (pool) {
+        cudaStreamSynchronize(stream);
+        cudaFree(pool);
+        pool = nullptr;
+        pool_bytes = 0;
+    }
+    size_t want = std::max(bytes, (size_t)64 << 20);
+    if (cudaMalloc(&pool, want) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NBG_ENOMEM, "device workspace of %zu bytes unavailable", want);
+    }
+    pool_bytes = want;
+    return NBG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batch construction
+
+static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
+    bb = BatchBuild();
+    if (count <= 0) return fail(NBG_EINVAL, "empty batch");
+    bb.prods.resize((size_t)count);
+    std::vector<int> npass((size_t)count);
+    int pmax = 1;
+    int bmin = 64;
+    size_t work = 0, aggw = 0;
+    std::vector<size_t> xa_off((size_t)count), xb_off((size_t)count), agg_off((size_t)count);
+    for (int64_t k = 0; k < count; k++) {
+        const ProdIn& q = in[k];
+        DProd& P = bb.prods[(size_t)k];
+        memset(&P, 0, sizeof P);
+        // magnitude bits must describe the buffers: the packer reads limb
+        // (bits-1)/64 at most.  A zero operand (no set bit) is the caller's
+        // case to handle, as NBig * does before reaching the engine.
+        if (q.bits_a < 1 || q.bits_a > 64 * q.m || (!q.sqr && (q.bits_b < 1 || q.bits_b > 64 * q.n)))
+            return fail(NBG_EINVAL, "product %lld: magnitude bits out of range (zero operand?)", (long long)k);
+        int bch;
+        int64_t N;
+        int rc = ntt_params(q.bits_a, q.sqr ? q.bits_a : q.bits_b, &bch, &N);
+        if (rc) return rc;
+        PlanRec* pr;
+        rc = E.get_plan(N, q.sqr, &pr);
+        if (rc) return rc;
+        P.a = q.a;
+        P.b = q.sqr ? q.a : q.b;
+        P.r = q.r;
+        P.m = q.m;
+        P.n = q.sqr ? q.m : q.n;
+        P.rn = P.m + P.n;
+        P.bch = bch;
+        P.sqr = q.sqr;
+        P.nca = (q.bits_a + bch - 1) / bch;
+        P.ncb = q.sqr ? P.nca : (q.bits_b + bch - 1) / bch;
+        P.nconv = P.nca + P.ncb - 1;
+        P.plan = pr->slot;
+        P.npass = pr->d.npass;
+        P.flags = 0;
+        P.ntl = (P.rn + UNPACK_TL - 1) / UNPACK_TL;
+        npass[(size_t)k] = P.npass;
+        pmax = std::max(pmax, P.npass);
+        bmin = std::min(bmin, bch);
+        xa_off[(size_t)k] = work;
+        work += 2 * (size_t)N;
+        if (P.npass > 1 && !P.sqr) {
+            xb_off[(size_t)k] = work;
+            work += 2 * (size_t)N;
+        } else {
+            xb_off[(size_t)k] = SIZE_MAX;
+        }
+        agg_off[(size_t)k] = aggw;
+        aggw += (size_t)P.ntl;
+        bb.plan_of.push_back(pr);
+    }
+    bb.work_doubles = work;
+    bb.agg_words = aggw;
+    bb.xa_off = xa_off;
+    bb.xb_off = xb_off;
+    bb.agg_off = agg_off;
+
+    // jobs per step (alignment: every product's pointwise pass runs in one launch)
+    std::vector<std::vector<Job>> fwd((size_t)std::max(pmax - 1, 0)), rev((size_t)std::max(pmax - 1, 0));
+    std::vector<Job> pwr, unp, car;
+    std::vector<size_t> fwd_smem(fwd.size(), 0), rev_smem(rev.size(), 0);
+    size_t pwr_smem = 0;
+    // algorithmic FP64 instructions per butterfly of the reference schedule
+    // (fwd, rev), counted on the oracle's restatement: radix-2 10, radix-3 32,
+    // radix-4 40, radix-5 94/98, radix-7 173/201; pointwise 7 per point; the
+    // Garner unpack 28 per coefficient.
+    auto bfly_ops = [](int m, bool fwd) -> double {
+        switch (m) {
+            case 2: return 10;
+            case 3: return 32;
+            case 4: return 40;
+            case 5: return fwd ? 94 : 98;
+            default: return fwd ? 173 : 201;
+        }
+    };
+    auto pass_ops = [&](const DPlan& pl, const DPass& ps, bool fwd) {
+        double o = 0;
+        for (int s = ps.sa; s <= ps.sb; s++) o += bfly_ops(pl.st[s].m, fwd) * (double)ps.G * ps.C / pl.st[s].m;
+        return o;
+    };
+    std::vector<double> fwd_ops(fwd.size(), 0), fwd_bytes(fwd.size(), 0), rev_ops(fwd.size(), 0),
+        rev_bytes(fwd.size(), 0);
+    double pwr_ops = 0, pwr_bytes = 0, unp_ops = 0, unp_bytes = 0;
+    for (int64_t k = 0; k < count; k++) {
+        const DProd& P = bb.prods[(size_t)k];
+        const DPlan& pl = bb.plan_of[(size_t)k]->d;
+        const int Pn = P.npass;
+        const double N = (double)pl.N;
+        const double ops_cnt = P.sqr ? 1.0 : 2.0;
+        for (int p = 0; p < Pn - 1; p++) {
+            const DPass& ps = pl.pass[p];
+            const size_t step = (size_t)(pmax - Pn + p);
+            fwd_ops[step] += 2.0 * ops_cnt * pass_ops(pl, ps, true) * (double)ps.ntiles;
+            const double in_b = p == 0 ? (double)(P.nca + (P.sqr ? 0 : P.ncb)) * P.bch / 8.0 * 2.0
+                                       : 2.0 * ops_cnt * 8.0 * N;
+            fwd_bytes[step] += in_b + 2.0 * ops_cnt * 8.0 * N;
+        }
+        {
+            const DPass& ps = pl.pass[Pn - 1];
+            pwr_ops += 2.0 * (ops_cnt * pass_ops(pl, ps, true) + 7.0 * ps.G + pass_ops(pl, ps, false)) * (double)ps.ntiles;
+            const double in_b = Pn == 1 ? (double)(P.nca + (P.sqr ? 0 : P.ncb)) * P.bch / 8.0 * 2.0
+                                        : 2.0 * ops_cnt * 8.0 * N;
+            pwr_bytes += in_b + 2.0 * 8.0 * N;
+        }
+        for (int p = Pn - 2; p >= 0; p--) {
+            const DPass& ps = pl.pass[p];
+            const size_t step = (size_t)(Pn - 2 - p);
+            rev_ops[step] += 2.0 * pass_ops(pl, ps, false) * (double)ps.ntiles;
+            rev_bytes[step] += 2.0 * 16.0 * N;
+        }
+        unp_ops += 28.0 * (double)P.nconv;
+        unp_bytes += 16.0 * (double)P.nconv + 8.0 * (double)P.rn;
+    }
+
+    for (int64_t k = 0; k < count; k++) {
+        const DProd& P = bb.prods[(size_t)k];
+        const DPlan& pl = bb.plan_of[(size_t)k]->d;
+        const int Pn = P.npass;
+        for (int p = 0; p < Pn - 1; p++) {
+            const DPass& ps = pl.pass[p];
+            const size_t step = (size_t)(pmax - Pn + p);
+            for (int f = 0; f < 2; f++)
+                for (int op = 0; op < (P.sqr ? 1 : 2); op++)
+                    for (int64_t t = 0; t < ps.ntiles; t++)
+                        fwd[step].push_back(Job{(int32_t)k, f | (op << 1) | (p << 8), t});
+            fwd_smem[step] = std::max(fwd_smem[step], sizeof(double) * (size_t)ps.G * (size_t)ps.C);
+        }
+        {
+            const DPass& ps = pl.pass[Pn - 1];
+            for (int f = 0; f < 2; f++)
+                for (int64_t t = 0; t < ps.ntiles; t++) pwr.push_back(Job{(int32_t)k, f | ((Pn - 1) << 8), t});
+            pwr_smem = std::max(pwr_smem, sizeof(double) * (size_t)ps.G * (size_t)ps.C * (P.sqr ? 1 : 2));
+        }
+        for (int p = Pn - 2; p >= 0; p--) {
+            const DPass& ps = pl.pass[p];
+            const size_t step = (size_t)(Pn - 2 - p);
+            for (int f = 0; f < 2; f++)
+                for (int64_t t = 0; t < ps.ntiles; t++) rev[step].push_back(Job{(int32_t)k, f | (p << 8), t});
+            rev_smem[step] = std::max(rev_smem[step], sizeof(double) * (size_t)ps.G * (size_t)ps.C);
+        }
+        for (int64_t t = 0; t < P.ntl; t++) unp.push_back(Job{(int32_t)k, 0, t});
+        if (P.ntl > 1) car.push_back(Job{(int32_t)k, 0, 0});
+    }
+    // biggest pointwise tiles first so the tail of the launch is short
+    std::stable_sort(pwr.begin(), pwr.end(), [&](const Job& x, const Job& y) {
+        const DPlan& px = bb.plan_of[(size_t)x.prod]->d;
+        const DPlan& py = bb.plan_of[(size_t)y.prod]->d;
+        return px.pass[bb.prods[(size_t)x.prod].npass - 1].G > py.pass[bb.prods[(size_t)y.prod].npass - 1].G;
+    });
+    auto add = [&](int kind, std::vector<Job>& v, size_t smem, double ops, double bytes) {
+        if (v.empty()) return;
+        Launch L{kind, (int64_t)bb.jobs.size(), (int64_t)v.size(), smem};
+        L.alg_ops = ops;
+        L.alg_bytes = bytes;
+        bb.launches.push_back(L);
+        bb.jobs.insert(bb.jobs.end(), v.begin(), v.end());
+    };
+    for (size_t s = 0; s < fwd.size(); s++) add(JK_FWD, fwd[s], fwd_smem[s], fwd_ops[s], fwd_bytes[s]);
+    add(JK_PWR, pwr, pwr_smem, pwr_ops, pwr_bytes);
+    for (size_t s = 0; s < rev.size(); s++) add(JK_REV, rev[s], rev_smem[s], rev_ops[s], rev_bytes[s]);
+    const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / bmin + 4;
+    add(JK_UNPACK, unp, sizeof(uint64_t) * 2 * (size_t)align_up((size_t)ncoef, 2), unp_ops, unp_bytes);
+    add(JK_CARRY, car, 0, 0.0, 4.0 * (double)car.size());
+    for (const Launch& L : bb.launches)
+        if ((int)L.smem > E.smem_optin) return fail(NBG_EINVAL, "tile needs %zu bytes of shared memory", L.smem);
+
+    // device layout: [prods | jobs | work | agg]
+    bb.off_prods = 0;
+    bb.off_jobs = align_up(sizeof(DProd) * (size_t)count, 256);
+    bb.off_work = align_up(bb.off_jobs + sizeof(Job) * bb.jobs.size(), 256);
+    bb.off_agg = align_up(bb.off_work + sizeof(double) * work, 256);
+    bb.dev_bytes = align_up(bb.off_agg + sizeof(uint32_t) * aggw, 256);
+    return NBG_OK;
+}
+
+// Point the descriptors at the device block and upload descriptors + jobs.
+int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st) {
+    double* work = (double*)(dbase + bb.off_work);
+    uint32_t* agg = (uint32_t*)(dbase + bb.off_agg);
+    for (size_t k = 0; k < bb.prods.size(); k++) {
+        DProd& P = bb.prods[k];
+        const int64_t N = bb.plan_of[k]->d.N;
+        P.xa[0] = work + bb.xa_off[k];
+        P.xa[1] = P.xa[0] + N;
+        if (bb.xb_off[k] != SIZE_MAX) {
+            P.xb[0] = work + bb.xb_off[k];
+            P.xb[1] = P.xb[0] + N;
+        } else {
+            P.xb[0] = P.xb[1] = nullptr;
+        }
+        P.agg = agg + bb.agg_off[k];
+    }
+    CUDA_TRY(cudaMemcpyAsync(dbase + bb.off_prods, bb.prods.data(), sizeof(DProd) * bb.prods.size(),
+                             cudaMemcpyHostToDevice, st));
+    if (!bb.jobs.empty())
+        CUDA_TRY(cudaMemcpyAsync(dbase + bb.off_jobs, bb.jobs.data(), sizeof(Job) * bb.jobs.size(),
+                                 cudaMemcpyHostToDevice, st));
+    (void)E;
+    return NBG_OK;
+}
+
+int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st) {
+    const DProd* prods = (const DProd*)(dbase + bb.off_prods);
+    const Job* jobs = (const Job*)(dbase + bb.off_jobs);
+    for (const Launch& L : bb.launches) {
+        cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, jobs + L.off, L.n, L.smem, 0, st);
+        if (e != cudaSuccess) return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n,
+                                          cudaGetErrorString(e));
+        g_launches++;
+    }
+    return NBG_OK;
+}
+
+}  // namespace nbg

@@ -1,0 +1,102 @@
+// engine.h — host engine internals shared by engine.cpp, api.cpp and serve.cpp.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "types.h"
+
+namespace nbg {
+
+int fail(int code, const char* fmt, ...);
+const char* last_error();
+extern std::atomic<int64_t> g_launches;
+
+int64_t magnitude_bits(const uint64_t* a, int64_t n);
+int64_t ntt_len(int64_t T);
+int ntt_params(int64_t bits_a, int64_t bits_b, int* b_out, int64_t* N_out);
+
+// Pass-split knobs (the autotuner's search space).
+struct Tuning {
+    int full_max_mul = 4096;  // one-pass (whole transform in shared memory) up to this N, products
+    int full_max_sqr = 8192;  // same for squares (one operand tile)
+    int last_max = 4096;      // largest contiguous block of the last pass
+    int early_gmax = 256;     // largest row count of an early (column) pass
+    int tile_target = 2048;   // target doubles per column-pass tile
+    int cmax = 128;           // most adjacent columns per column-pass tile
+    std::string to_json() const;
+    int from_json(const char* js);
+};
+
+int plan_structure(int64_t N, int for_sqr, const Tuning& tun, DPlan& d);
+
+struct PlanRec {
+    DPlan d;
+    double* dtab = nullptr;
+    size_t table_bytes = 0;
+    int slot = -1;
+};
+
+struct Engine {
+    bool ready = false;
+    int dev = -1;
+    int num_sms = 0;
+    int smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    std::recursive_mutex mu;
+    Tuning tun;
+    std::map<int64_t, PlanRec> plans;
+    std::vector<double*> graveyard;
+    DPlan* d_plans = nullptr;
+    int plan_cap = 4096;
+    int plan_used = 0;
+    void* pool = nullptr;
+    size_t pool_bytes = 0;
+
+    int init(int device);
+    int ensure();
+    int build_plan(int64_t N, PlanRec& pr, int for_sqr);
+    int get_plan(int64_t N, int for_sqr, PlanRec** out);
+    void drop_plans();
+    int ensure_pool(size_t bytes);
+};
+extern Engine g_eng;
+
+// One product as the batch builder sees it (device pointers).
+struct ProdIn {
+    const uint64_t* a;
+    const uint64_t* b;
+    uint64_t* r;
+    int64_t m, n;
+    int64_t bits_a, bits_b;
+    int sqr;
+};
+
+struct Launch {
+    int kind;
+    int64_t off, n;
+    size_t smem;
+    double alg_ops = 0;    // FP64 instructions of the reference schedule done by this launch
+    double alg_bytes = 0;  // compulsory global bytes (operand/limb reads, tile loads and stores)
+};
+
+struct BatchBuild {
+    std::vector<DProd> prods;
+    std::vector<PlanRec*> plan_of;
+    std::vector<Job> jobs;
+    std::vector<Launch> launches;
+    std::vector<size_t> xa_off, xb_off, agg_off;
+    size_t work_doubles = 0, agg_words = 0;
+    size_t off_prods = 0, off_jobs = 0, off_work = 0, off_agg = 0, dev_bytes = 0;
+};
+
+int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb);
+int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st);
+int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st);
+
+}  // namespace nbg

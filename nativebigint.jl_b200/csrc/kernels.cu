@@ -1,0 +1,551 @@
+// kernels.cu — the fp-NTT product pipeline on sm_100a FP64 cores.
+//
+// Kernels (each is a work-queue launch: CTA i takes Job i of a host-built list
+// that may mix products of any size):
+//   k_fwd     forward pass of one tile; pass 0 packs limbs into b-bit chunks
+//             on load (fp_ntt_pack!, src/fpntt.jl:744-768)
+//   k_pwr     last pass: forward stages, pointwise product
+//             (fp_ntt_pointwise!, :770-785) and the reverse's first stages on
+//             the same shared-memory block; packs on load for one-pass products
+//   k_rev     reverse pass of one tile (fp_ntt_rev!, :727-733)
+//   k_unpack  Garner CRT (fp_unpack_coeff, :806-816) and limb assembly of a
+//             1024-limb output tile with a block-wide carry-lookahead scan
+//   k_carry   cross-tile carry scan and fix-up, one CTA per product
+//   k_twiddle expands exact minimal-balanced twiddle tables from two small
+//             power tables (twiddle values are unique residues, so any exact
+//             construction equals fp_twiddles, :173-186)
+#include <cuda_runtime.h>
+
+#include "butterfly.cuh"
+#include "kernels.h"
+
+namespace nbg {
+
+__constant__ Fp c_fp[2];
+__constant__ double c_garner[2];  // g = p1^-1 mod p2 (canonical) and g/p2
+
+__device__ __forceinline__ Fp fpctx(int f) { return c_fp[f]; }
+
+// ---------------------------------------------------------------------------
+// Pack: chunk i of an n-limb operand (fp_ntt_pack!, :744-768).  The
+// reference's fast loop always ORs in the next limb; its high bits are masked
+// off unless sh + b > 64, so this single form is identical.
+__device__ __forceinline__ double pack_chunk(const uint64_t* __restrict__ limbs, int64_t n, int b, int64_t nch,
+                                             int64_t i) {
+    if (i >= nch) return 0.0;
+    int64_t bit = i * (int64_t)b;
+    int64_t w = bit >> 6;
+    int sh = (int)(bit & 63);
+    uint64_t c = __ldg(limbs + w) >> sh;
+    if (sh + b > 64 && w + 1 < n) c |= __ldg(limbs + w + 1) << (64 - sh);
+    return (double)(c & ((1ULL << b) - 1ULL));
+}
+
+// ---------------------------------------------------------------------------
+// One stage over a shared-memory tile of G rows x C columns (row stride C).
+// Local stage geometry: Lloc = L_s/Qb rows per block, Qloc = Q_s/Qb.
+template <int M, bool FWD>
+__device__ __forceinline__ void stage_tile(double* __restrict__ s, int G, int lc, int Lloc, int Qloc,
+                                           const double* __restrict__ tw, int64_t Qs, int64_t Qb, int64_t j0,
+                                           const double* rot, Fp F) {
+    const int C = 1 << lc;
+    const int nb = (G / M) << lc;
+    const int stride = Qloc << lc;
+    double r[8];
+#pragma unroll
+    for (int t = 0; t < 8; t++) r[t] = rot[t];
+    for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+        int c = e & (C - 1);
+        int row = e >> lc;
+        int blk = row / Qloc;
+        int jl = row - blk * Qloc;
+        int base = ((blk * Lloc + jl) << lc) + c;
+        double y[M];
+#pragma unroll
+        for (int t = 0; t < M; t++) y[t] = s[base + t * stride];
+        if constexpr (M == 2) {
+            butterfly2(y[0], y[1], F);
+        } else {
+            double w[M];
+            int64_t j = (int64_t)jl * Qb + j0 + c;
+            w[0] = 0.0;
+#pragma unroll
+            for (int t = 1; t < M; t++) w[t] = __ldg(tw + (int64_t)(t - 1) * Qs + j);
+            butterfly<M, FWD>(y, w, r, F);
+        }
+#pragma unroll
+        for (int t = 0; t < M; t++) s[base + t * stride] = y[t];
+    }
+}
+
+template <bool FWD>
+__device__ void run_stage(double* s, const DStage& st, int f, int G, int lc, int64_t Qb, int64_t j0) {
+    const Fp F = fpctx(f);
+    const int Lloc = (int)(st.L / Qb);
+    const int Qloc = (int)(st.Q / Qb);
+    switch (st.m) {
+        case 2: stage_tile<2, FWD>(s, G, lc, Lloc, Qloc, nullptr, st.Q, Qb, j0, st.rot[f], F); break;
+        case 3: stage_tile<3, FWD>(s, G, lc, Lloc, Qloc, st.tw[f], st.Q, Qb, j0, st.rot[f], F); break;
+        case 4: stage_tile<4, FWD>(s, G, lc, Lloc, Qloc, st.tw[f], st.Q, Qb, j0, st.rot[f], F); break;
+        case 5: stage_tile<5, FWD>(s, G, lc, Lloc, Qloc, st.tw[f], st.Q, Qb, j0, st.rot[f], F); break;
+        default: stage_tile<7, FWD>(s, G, lc, Lloc, Qloc, st.tw[f], st.Q, Qb, j0, st.rot[f], F); break;
+    }
+}
+
+template <bool FWD>
+__device__ void run_pass(double* s, const DPlan& pl, const DPass& ps, int f, int64_t j0) {
+    const int lc = __ffs(ps.C) - 1;
+    if (FWD) {
+        for (int i = ps.sa; i <= ps.sb; i++) {
+            __syncthreads();
+            run_stage<true>(s, pl.st[i], f, ps.G, lc, ps.Qb, j0);
+        }
+    } else {
+        for (int i = ps.sb; i >= ps.sa; i--) {
+            __syncthreads();
+            run_stage<false>(s, pl.st[i], f, ps.G, lc, ps.Qb, j0);
+        }
+    }
+    __syncthreads();
+}
+
+// Tile geometry: tile t -> block offset o_a (multiple of L_sa) and first column j0.
+struct TileGeo {
+    int64_t base;  // o_a + j0
+    int64_t j0;
+};
+__device__ __forceinline__ TileGeo tile_geo(const DPlan& pl, const DPass& ps, int64_t t) {
+    int64_t per = ps.Qb / ps.C;
+    int64_t blk = t / per;
+    int64_t jc = t - blk * per;
+    TileGeo g;
+    g.j0 = jc * ps.C;
+    g.base = blk * pl.st[ps.sa].L + g.j0;
+    return g;
+}
+
+__device__ __forceinline__ void load_tile(double* s, const double* __restrict__ x, const DPass& ps, int64_t base) {
+    const int lc = __ffs(ps.C) - 1;
+    const int n = ps.G << lc;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        int k = e >> lc, c = e & (ps.C - 1);
+        s[e] = x[base + c + (int64_t)k * ps.Qb];
+    }
+}
+__device__ __forceinline__ void store_tile(const double* s, double* __restrict__ x, const DPass& ps, int64_t base) {
+    const int lc = __ffs(ps.C) - 1;
+    const int n = ps.G << lc;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        int k = e >> lc, c = e & (ps.C - 1);
+        x[base + c + (int64_t)k * ps.Qb] = s[e];
+    }
+}
+__device__ __forceinline__ void pack_tile(double* s, const uint64_t* limbs, int64_t n, int b, int64_t nch,
+                                          const DPass& ps, int64_t base) {
+    const int lc = __ffs(ps.C) - 1;
+    const int cnt = ps.G << lc;
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+        int k = e >> lc, c = e & (ps.C - 1);
+        s[e] = pack_chunk(limbs, n, b, nch, base + c + (int64_t)k * ps.Qb);
+    }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_fwd(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
+                                             const Job* __restrict__ jobs, int64_t njobs) {
+    extern __shared__ double smem[];
+    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+        const Job jb = jobs[ji];
+        const DProd& P = prods[jb.prod];
+        const DPlan& pl = plans[P.plan];
+        const int f = jb.sub & 1, opb = (jb.sub >> 1) & 1, pass = (jb.sub >> 8) & 0xff;
+        const DPass& ps = pl.pass[pass];
+        const TileGeo g = tile_geo(pl, ps, jb.tile);
+        double* x = opb ? P.xb[f] : P.xa[f];
+        __syncthreads();
+        if (pass == 0 && !(P.flags & PF_PRELOADED)) {
+            if (opb) pack_tile(smem, P.b, P.n, P.bch, P.ncb, ps, g.base);
+            else pack_tile(smem, P.a, P.m, P.bch, P.nca, ps, g.base);
+        } else {
+            load_tile(smem, x, ps, g.base);
+        }
+        run_pass<true>(smem, pl, ps, f, g.j0);
+        store_tile(smem, x, ps, g.base);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_pwr(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
+                                             const Job* __restrict__ jobs, int64_t njobs) {
+    extern __shared__ double smem[];
+    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+        const Job jb = jobs[ji];
+        const DProd& P = prods[jb.prod];
+        const DPlan& pl = plans[P.plan];
+        const int f = jb.sub & 1;
+        const int pass = P.npass - 1;
+        const DPass& ps = pl.pass[pass];
+        const TileGeo g = tile_geo(pl, ps, jb.tile);
+        const int cnt = ps.G * ps.C;
+        double* sa = smem;
+        double* sb = smem + cnt;
+        __syncthreads();
+        if (pass == 0 && !(P.flags & PF_PRELOADED)) {
+            pack_tile(sa, P.a, P.m, P.bch, P.nca, ps, g.base);
+            if (!P.sqr) pack_tile(sb, P.b, P.n, P.bch, P.ncb, ps, g.base);
+        } else {
+            load_tile(sa, P.xa[f], ps, g.base);
+            if (!P.sqr) load_tile(sb, P.xb[f], ps, g.base);
+        }
+        run_pass<true>(sa, pl, ps, f, g.j0);
+        if (!P.sqr) run_pass<true>(sb, pl, ps, f, g.j0);
+        const Fp F = fpctx(f);
+        if (P.sqr) {
+            for (int e = threadIdx.x; e < cnt; e += blockDim.x) sa[e] = fp_mulmod(sa[e], sa[e], F);
+        } else {
+            for (int e = threadIdx.x; e < cnt; e += blockDim.x) sa[e] = fp_mulmod(sa[e], sb[e], F);
+        }
+        run_pass<false>(sa, pl, ps, f, g.j0);
+        store_tile(sa, P.xa[f], ps, g.base);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_rev(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
+                                             const Job* __restrict__ jobs, int64_t njobs) {
+    extern __shared__ double smem[];
+    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+        const Job jb = jobs[ji];
+        const DProd& P = prods[jb.prod];
+        const DPlan& pl = plans[P.plan];
+        const int f = jb.sub & 1, pass = (jb.sub >> 8) & 0xff;
+        const DPass& ps = pl.pass[pass];
+        const TileGeo g = tile_geo(pl, ps, jb.tile);
+        __syncthreads();
+        load_tile(smem, P.xa[f], ps, g.base);
+        run_pass<false>(smem, pl, ps, f, g.j0);
+        store_tile(smem, P.xa[f], ps, g.base);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Unpack.  Coefficient i (value c_i = c1 + p1*u < p1*p2 < 2^100) sits at
+// x[(N - i) mod N] scaled by N (fp_ntt_rev! :723-726).  The product is
+// sum_i c_i 2^(b i); its limb w collects the 64-bit slices of the (at most
+// five) coefficients overlapping bits [64w, 64w+64).  This equals the
+// reference's S1 + p1*S2 fold (:793-795, :923) as an integer, so the limbs are
+// identical.
+__device__ __forceinline__ void garner(const double* __restrict__ x1, const double* __restrict__ x2, int64_t idx,
+                                       const DPlan& pl, uint64_t& lo, uint64_t& hi) {
+    const Fp F1 = fpctx(0), F2 = fpctx(1);
+    double v1 = fp_mulmod4(__ldg(x1 + idx), pl.ninv[0], pl.ninvp[0], F1);
+    v1 = v1 < 0.0 ? dadd(v1, F1.p) : v1;
+    double v2 = fp_mulmod4(__ldg(x2 + idx), pl.ninv[1], pl.ninvp[1], F2);
+    double u = fp_mulmod4(dsub(v2, fp_reduce(v1, F2)), c_garner[0], c_garner[1], F2);
+    uint64_t c1 = (uint64_t)v1;
+    uint64_t uu = (uint64_t)(u < 0.0 ? dadd(u, F2.p) : u);
+    // c = c1 + p1*uu  (128-bit)
+    uint64_t plo = uu * P1_U;
+    uint64_t phi = __umul64hi(uu, P1_U);
+    lo = plo + c1;
+    hi = phi + (lo < plo ? 1ULL : 0ULL);
+}
+
+// 64-bit slice of c * 2^d for d in [-127, 63]
+__device__ __forceinline__ uint64_t slice64(uint64_t lo, uint64_t hi, int d) {
+    if (d >= 0) return d == 0 ? lo : (lo << d);
+    int s = -d;
+    if (s >= 64) return s == 64 ? hi : (hi >> (s - 64));
+    return (lo >> s) | (hi << (64 - s));
+}
+
+constexpr int UNPACK_THREADS = 256;
+constexpr int LIMBS_PER_THREAD = UNPACK_TL / UNPACK_THREADS;
+
+__device__ __forceinline__ uint32_t gp_compose(uint32_t lower, uint32_t upper) {
+    // (g,p) pairs packed as bit0 = generate, bit1 = propagate; lower then upper.
+    uint32_t g = (upper & 1u) | ((upper >> 1) & lower & 1u);
+    uint32_t p = (upper >> 1) & (lower >> 1) & 1u;
+    return g | (p << 1);
+}
+
+// Limb value V_w = sum of slices; returns lo, sets hi (<= 4).
+__device__ __forceinline__ uint64_t limb_sum(const uint64_t* __restrict__ clo, const uint64_t* __restrict__ chi,
+                                             int64_t ibase, int64_t ilo, int64_t ihi, int b, int64_t w,
+                                             uint64_t& hiout) {
+    int64_t a = 64 * w - 99;
+    int64_t i0 = a <= 0 ? 0 : (a + b - 1) / b;
+    int64_t i1 = (64 * w + 63) / b;
+    if (i0 < ilo) i0 = ilo;
+    if (i1 > ihi) i1 = ihi;
+    uint64_t lo = 0, hi = 0;
+    for (int64_t i = i0; i <= i1; i++) {
+        int d = (int)(i * b - 64 * w);
+        uint64_t sl = slice64(clo[i - ibase], chi[i - ibase], d);
+        lo += sl;
+        hi += (lo < sl) ? 1ULL : 0ULL;
+    }
+    hiout = hi;
+    return lo;
+}
+
+__global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restrict__ prods,
+                                                           const DPlan* __restrict__ plans,
+                                                           const Job* __restrict__ jobs, int64_t njobs) {
+    extern __shared__ uint64_t usm[];
+    __shared__ uint32_t wagg[UNPACK_THREADS / 32];
+    __shared__ uint64_t hilast[UNPACK_THREADS + 1];
+    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+        const Job jb = jobs[ji];
+        const DProd& P = prods[jb.prod];
+        const DPlan& pl = plans[P.plan];
+        const int b = P.bch;
+        const int64_t N = pl.N;
+        const int64_t w0 = jb.tile * UNPACK_TL;
+        const int64_t w1 = min(w0 + (int64_t)UNPACK_TL, P.rn);
+        const int64_t wlo = w0 > 0 ? w0 - 1 : 0;
+        int64_t ilo = 64 * wlo - 99;
+        ilo = ilo <= 0 ? 0 : (ilo + b - 1) / b;
+        int64_t ihi = (64 * (w1 - 1) + 63) / b;
+        if (ihi > P.nconv - 1) ihi = P.nconv - 1;
+        const int64_t ncoef = ihi >= ilo ? ihi - ilo + 1 : 0;
+        uint64_t* clo = usm;
+        uint64_t* chi = usm + ((ncoef + 1) & ~1LL);
+        __syncthreads();
+        for (int64_t k = threadIdx.x; k < ncoef; k += blockDim.x) {
+            int64_t i = ilo + k;
+            int64_t idx = i == 0 ? 0 : N - i;
+            uint64_t lo, hi;
+            garner(P.xa[0], P.xa[1], idx, pl, lo, hi);
+            clo[k] = lo;
+            chi[k] = hi;
+        }
+        __syncthreads();
+        // limb sums for this thread's LIMBS_PER_THREAD consecutive limbs
+        const int t = threadIdx.x;
+        uint64_t lo[LIMBS_PER_THREAD], hiv[LIMBS_PER_THREAD];
+#pragma unroll
+        for (int q = 0; q < LIMBS_PER_THREAD; q++) {
+            int64_t w = w0 + (int64_t)t * LIMBS_PER_THREAD + q;
+            if (w < w1) lo[q] = limb_sum(clo, chi, ilo, ilo, ihi, b, w, hiv[q]);
+            else { lo[q] = 0; hiv[q] = 0; }
+        }
+        hilast[t + 1] = hiv[LIMBS_PER_THREAD - 1];
+        if (t == 0) {
+            uint64_t h0 = 0;
+            if (w0 > 0) (void)limb_sum(clo, chi, ilo, ilo, ihi, b, w0 - 1, h0);
+            hilast[0] = h0;
+        }
+        __syncthreads();
+        // resolve the slice-sum overflow: t_w = lo_w + hi_{w-1} -> (lo', generate)
+        uint64_t hin = hilast[t];
+        uint32_t gpq[LIMBS_PER_THREAD];
+        uint32_t agg = 2u;  // identity: propagate, no generate
+#pragma unroll
+        for (int q = 0; q < LIMBS_PER_THREAD; q++) {
+            int64_t w = w0 + (int64_t)t * LIMBS_PER_THREAD + q;
+            uint64_t v = lo[q] + hin;
+            uint32_t g = v < hin ? 1u : 0u;
+            hin = hiv[q];
+            lo[q] = v;
+            uint32_t p = (v == ~0ULL) ? 1u : 0u;
+            gpq[q] = (w < w1) ? (g | (p << 1)) : 2u;
+            agg = gp_compose(agg, gpq[q]);
+        }
+        // block exclusive scan of agg (carry-in to each thread, tile carry-in 0)
+        const int lane = t & 31, wid = t >> 5;
+        uint32_t incl = agg;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl = gp_compose(o, incl);
+        }
+        if (lane == 31) wagg[wid] = incl;
+        __syncthreads();
+        uint32_t wpre = 2u;
+        for (int k = 0; k < wid; k++) wpre = gp_compose(wpre, wagg[k]);
+        uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) excl = 2u;
+        excl = gp_compose(wpre, excl);
+        uint32_t cin = excl & 1u;  // tile carry-in assumed 0
+#pragma unroll
+        for (int q = 0; q < LIMBS_PER_THREAD; q++) {
+            int64_t w = w0 + (int64_t)t * LIMBS_PER_THREAD + q;
+            uint64_t out = lo[q] + cin;
+            cin = (gpq[q] & 1u) | ((gpq[q] >> 1) & cin);
+            if (w < w1) P.r[w] = out;
+        }
+        if (t == blockDim.x - 1 && P.agg) {
+            uint32_t tot = 2u;
+            for (int k = 0; k < UNPACK_THREADS / 32; k++) tot = gp_compose(tot, wagg[k]);
+            P.agg[jb.tile] = tot;
+        }
+    }
+}
+
+// Cross-tile carries: one CTA per product.  Each thread composes a run of
+// tile aggregates, the block scans them, and every tile whose true carry-in is
+// 1 gets +1 propagated from its first limb (limbs equal to 2^64-1 wrap to 0).
+__global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, const Job* __restrict__ jobs,
+                                               int64_t njobs) {
+    __shared__ uint32_t wagg[8];
+    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+        const DProd& P = prods[jobs[ji].prod];
+        const int64_t nt = P.ntl;
+        const int t = threadIdx.x;
+        const int64_t per = (nt + blockDim.x - 1) / blockDim.x;
+        const int64_t t0 = (int64_t)t * per, t1 = min(t0 + per, nt);
+        uint32_t agg = 2u;
+        for (int64_t k = t0; k < t1; k++) agg = gp_compose(agg, P.agg[k]);
+        const int lane = t & 31, wid = t >> 5;
+        uint32_t incl = agg;
+        for (int off = 1; off < 32; off <<= 1) {
+            uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl = gp_compose(o, incl);
+        }
+        __syncthreads();
+        if (lane == 31) wagg[wid] = incl;
+        __syncthreads();
+        uint32_t wpre = 2u;
+        for (int k = 0; k < wid; k++) wpre = gp_compose(wpre, wagg[k]);
+        uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) excl = 2u;
+        excl = gp_compose(wpre, excl);
+        uint32_t cin = excl & 1u;
+        for (int64_t k = t0; k < t1; k++) {
+            uint32_t a = P.agg[k];
+            if (cin) {
+                int64_t w = k * UNPACK_TL, we = min(w + (int64_t)UNPACK_TL, P.rn);
+                while (w < we && P.r[w] == ~0ULL) { P.r[w] = 0; w++; }
+                if (w < we) P.r[w] += 1;
+            }
+            cin = (a & 1u) | ((a >> 1) & cin);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Standalone pack and pointwise (the transform-level entry points).
+__global__ void k_pack(double* __restrict__ x, int64_t N, const uint64_t* __restrict__ limbs, int64_t n, int b,
+                       int64_t nch) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = pack_chunk(limbs, n, b, nch, i);
+}
+__global__ void k_pointwise(double* __restrict__ xa, const double* __restrict__ xb, int64_t N, int f) {
+    const Fp F = fpctx(f);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        xa[i] = fp_mulmod(xa[i], xb[i], F);
+}
+// top-limb bit lengths for device batches: bits[2k] / bits[2k+1] of operand a / b
+__global__ void k_topbits(const DProd* __restrict__ prods, int64_t count, int64_t* __restrict__ bits) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < count; k += (int64_t)gridDim.x * blockDim.x) {
+        const DProd& P = prods[k];
+        uint64_t ta = P.a[P.m - 1];
+        bits[2 * k] = 64 * (P.m - 1) + (ta ? 64 - __clzll((long long)ta) : 0);
+        uint64_t tb = P.b[P.n - 1];
+        bits[2 * k + 1] = 64 * (P.n - 1) + (tb ? 64 - __clzll((long long)tb) : 0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Twiddle tables: tw[(t-1)*Q + j] = omega^e, e = (N/L)*t*j (< N), as
+//   minbal(mulmod(HI[e >> 12], LO[e & 4095]))
+// where HI/LO are exact minimal-balanced powers built on the host.  Both
+// factors are <= p/2, so the mulmod is exact and |r| < p; minbal then yields
+// the unique representative in [-p/2, p/2], the value fp_twiddles stores.
+__global__ void k_twiddle(double* __restrict__ out, int m, int64_t Q, int64_t step, const double* __restrict__ hi,
+                          const double* __restrict__ lo, int f) {
+    const Fp F = fpctx(f);
+    const int64_t total = (int64_t)(m - 1) * Q;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int64_t t = idx / Q + 1, j = idx - (t - 1) * Q;
+        int64_t e = step * t * j;
+        double v = fp_mulmod(hi[e >> 12], lo[e & 4095], F);
+        out[idx] = fp_minbal(v, F);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launch helpers
+
+static int g_smem_optin = 0;
+
+cudaError_t kernels_init(double p1, double p2) {
+    Fp h[2] = {{p1, 1.0 / p1}, {p2, 1.0 / p2}};
+    cudaError_t e = cudaMemcpyToSymbol(c_fp, h, sizeof h);
+    if (e != cudaSuccess) return e;
+    // Garner constant g = p1^-1 mod p2 (canonical) and g/p2 (fpntt.jl:879-880)
+    const uint64_t P1 = P1_U, P2 = P2_U;
+    // invmod by Fermat with 128-bit products
+    unsigned __int128 r = 1, a = P1 % P2;
+    uint64_t ex = P2 - 2;
+    while (ex) {
+        if (ex & 1) r = (r * a) % P2;
+        a = (a * a) % P2;
+        ex >>= 1;
+    }
+    double g[2];
+    g[0] = (double)(uint64_t)r;
+    g[1] = g[0] / p2;
+    e = cudaMemcpyToSymbol(c_garner, g, sizeof g);
+    if (e != cudaSuccess) return e;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const void* ks[] = {(const void*)k_fwd, (const void*)k_pwr, (const void*)k_rev, (const void*)k_unpack};
+    for (const void* k : ks) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, g_smem_optin);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+int kernels_smem_optin() { return g_smem_optin; }
+
+cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const Job* jobs, int64_t njobs,
+                        size_t smem, int grid_cap, cudaStream_t st) {
+    if (njobs <= 0) return cudaSuccess;
+    int64_t grid64 = njobs;
+    if (grid_cap > 0 && grid64 > grid_cap) grid64 = grid_cap;
+    if (grid64 > 0x7fffffff) grid64 = 0x7fffffff;
+    const unsigned grid = (unsigned)grid64;
+    switch (kind) {
+        case JK_FWD: k_fwd<<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_PWR: k_pwr<<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_REV: k_rev<<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_UNPACK: k_unpack<<<grid, UNPACK_THREADS, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_CARRY: k_carry<<<grid, 256, 0, st>>>(prods, jobs, njobs); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+static unsigned grid_for(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    if (b > 148 * 32) b = 148 * 32;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+cudaError_t launch_pack(double* x, int64_t N, const uint64_t* limbs, int64_t n, int b, int64_t nch, cudaStream_t st) {
+    k_pack<<<grid_for(N), 256, 0, st>>>(x, N, limbs, n, b, nch);
+    return cudaGetLastError();
+}
+cudaError_t launch_pointwise(double* xa, const double* xb, int64_t N, int f, cudaStream_t st) {
+    k_pointwise<<<grid_for(N), 256, 0, st>>>(xa, xb, N, f);
+    return cudaGetLastError();
+}
+cudaError_t launch_topbits(const DProd* prods, int64_t count, int64_t* bits, cudaStream_t st) {
+    k_topbits<<<grid_for(count), 256, 0, st>>>(prods, count, bits);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_twiddle(double* out, int m, int64_t Q, int64_t step, const double* hi, const double* lo, int f,
+                           cudaStream_t st) {
+    int64_t total = (int64_t)(m - 1) * Q;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (blocks < 1) blocks = 1;
+    k_twiddle<<<(unsigned)blocks, 256, 0, st>>>(out, m, Q, step, hi, lo, f);
+    return cudaGetLastError();
+}
+
+}  // namespace nbg

@@ -1,0 +1,25 @@
+// kernels.h — host-side entry points of kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "types.h"
+
+namespace nbg {
+
+// Uploads the prime constants and raises the kernels' dynamic shared-memory cap.
+cudaError_t kernels_init(double p1, double p2);
+int kernels_smem_optin();
+
+// One work-queue launch of `kind` (JobKind) over jobs[0..njobs).
+cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const Job* jobs, int64_t njobs,
+                        size_t smem, int grid_cap, cudaStream_t st);
+
+// Expands one stage's twiddle table (see k_twiddle).
+cudaError_t launch_twiddle(double* out, int m, int64_t Q, int64_t step, const double* hi, const double* lo, int f,
+                           cudaStream_t st);
+
+cudaError_t launch_pack(double* x, int64_t N, const uint64_t* limbs, int64_t n, int b, int64_t nch, cudaStream_t st);
+cudaError_t launch_pointwise(double* xa, const double* xb, int64_t N, int f, cudaStream_t st);
+cudaError_t launch_topbits(const DProd* prods, int64_t count, int64_t* bits, cudaStream_t st);
+
+}  // namespace nbg

@@ -1,0 +1,88 @@
+// types.h — plan, product and job descriptors shared by host and device code.
+//
+// A transform of length N = m*2^k is the reference's flat stage list
+// (src/fpntt.jl:236-271): odd Winograd stages 7,5,3,3 (those dividing m), the
+// radix-4 tower, and a twiddle-free radix-2 stage when k is odd.  Stage s has
+// span L_s (its butterflies run inside L_s-blocks) and stride Q_s = L_s/m_s;
+// its twiddle for lane t, column j is omega^((N/L_s)*t*j) in minimal balanced
+// form, stored t-major: tw[(t-1)*Q_s + j].
+//
+// On the GPU a contiguous run of stages [sa, sb] is one *pass*: every pass
+// tile is G = L_sa/Q_sb rows by C adjacent columns of stride Qb = Q_sb, held in
+// shared memory while all the pass's butterflies run.  The last pass always has
+// Qb = 1 (a contiguous G-block), so the pointwise product and the reverse's
+// first pass run on the same tile.
+#pragma once
+#include <cstdint>
+
+namespace nbg {
+
+constexpr int MAXST = 24;    // 4 odd + 17 radix-4 + radix-2 at N = 315*2^34
+constexpr int MAXPASS = MAXST;
+
+struct DStage {
+    int32_t m;           // radix 2, 3, 4, 5, 7
+    int32_t pad_;
+    int64_t L;           // span
+    int64_t Q;           // L / m
+    const double* tw[2]; // per prime, (m-1)*Q doubles (null for radix-2)
+    double rot[2][8];    // per prime combine constants (radix-4: rot[0] = wi)
+};
+
+struct DPass {
+    int32_t sa, sb;      // stage range, inclusive
+    int32_t G;           // rows per tile = L_sa / Q_sb
+    int32_t C;           // columns per tile (power of two dividing Qb)
+    int64_t Qb;          // column stride = Q_sb
+    int64_t ntiles;      // (N / L_sa) * (Qb / C)
+};
+
+struct DPlan {
+    int64_t N;
+    int32_t nst, npass;
+    double ninv[2], ninvp[2]; // 1/N mod p (minimal balanced) and ninv/p
+    DStage st[MAXST];
+    DPass pass[MAXPASS];
+};
+
+// One product r[0..rn) = a[0..m) * b[0..n) (b == a for a square).
+struct DProd {
+    const uint64_t* a;
+    const uint64_t* b;
+    uint64_t* r;
+    int64_t m, n, rn;
+    int64_t nca, ncb, nconv;
+    int32_t bch;         // chunk width in bits
+    int32_t sqr;         // 1: square (one operand transform per prime)
+    int32_t plan;        // index into the device plan array
+    int32_t npass;
+    int32_t flags;       // PF_* bits
+    int32_t pad_;
+    double* xa[2];       // per-prime transform buffers of operand a (and the result)
+    double* xb[2];       // per-prime buffers of operand b (multi-pass products only)
+    uint32_t* agg;       // per limb-tile carry aggregates (bit0 generate, bit1 propagate)
+    int64_t ntl;         // number of limb tiles
+};
+
+// Work item of one launch.  kind-specific meaning of `sub`:
+//   bit 0 prime, bit 1 operand (0 = a, 1 = b); pass index in bits 8..15.
+struct Job {
+    int32_t prod;
+    int32_t sub;
+    int64_t tile;
+};
+
+enum JobKind : int32_t {
+    JK_FWD = 0,   // forward pass (pass 0 packs limbs on load)
+    JK_PWR = 1,   // last pass: forward, pointwise, reverse (packs when npass == 1)
+    JK_REV = 2,   // reverse pass
+    JK_UNPACK = 3,// Garner + limb assembly + in-tile carries
+    JK_CARRY = 4, // cross-tile carry scan and fix-up (one job per product)
+};
+
+constexpr int UNPACK_TL = 1024;  // output limbs per unpack tile
+
+// DProd.flags
+constexpr int32_t PF_PRELOADED = 1;  // pass 0 loads xa/xb as-is instead of packing limbs
+
+}  // namespace nbg

@@ -1,0 +1,201 @@
+"""Host-side checks of libnbgpu.so that need no GPU: the library loads,
+exports every symbol include/nbgpu.h declares, its admission restatement
+agrees with the oracle, and argument errors come back as status codes."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import nbgpu
+import oracle as O
+from conftest import ROOT, rand_limbs
+
+
+def _declared_symbols() -> list[str]:
+    src = open(os.path.join(ROOT, "include", "nbgpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(nbg_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = nbgpu.lib()
+    syms = _declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) == set(nbgpu.EXPORTS)
+
+
+def test_library_is_sm100a_build():
+    # the fatbin must hold sm_100a code; check the ELF for the arch tag string
+    data = open(nbgpu.LIB_PATH, "rb").read()
+    assert b"sm_100a" in data
+
+
+def test_ntt_len_matches_oracle():
+    for T in list(range(1, 5000, 7)) + [15 << 14, (15 << 14) + 1, 7 << 10, 9 << 10, (1 << 34) + 1,
+                                       33 << 34, 53 << 34, 315 << 34]:
+        assert nbgpu.ntt_len(T) == O.ntt_len(T)
+    with pytest.raises(nbgpu.LengthError):
+        nbgpu.ntt_len((315 << 34) + 1)
+
+
+def test_ntt_params_matches_oracle():
+    rng = np.random.default_rng(11)
+    cases = [(1, 1), (64, 64), (64 * 4096, 64 * 4096), (64 * 2**24, 64 * 2**24), (9728, 64 * 65536)]
+    cases += [(int(rng.integers(1, 2**28)), int(rng.integers(1, 2**28))) for _ in range(2000)]
+    for ba, bb in cases:
+        assert nbgpu.ntt_params(ba, bb) == O.ntt_params(ba, bb)
+
+
+def test_magnitude_bits():
+    rng = np.random.default_rng(12)
+    for n in (1, 2, 5, 100):
+        a = rand_limbs(rng, n)
+        assert nbgpu.magnitude_bits(a) == O.magnitude_bits(a) == O.to_int(a).bit_length()
+
+
+def test_argument_errors_without_device():
+    L = nbgpu.lib()
+    r = np.zeros(4, dtype=np.uint64)
+    a = np.ones(2, dtype=np.uint64)
+    assert L.nbg_mul(r.ctypes.data, a.ctypes.data, 2, None, 2) == nbgpu.NBG_EINVAL
+    assert L.nbg_mul(r.ctypes.data, a.ctypes.data, 0, a.ctypes.data, 2) == nbgpu.NBG_EINVAL
+    # r aliasing an operand is rejected (src/fpntt.jl:979-981)
+    assert L.nbg_mul(a.ctypes.data, a.ctypes.data, 2, a.ctypes.data, 2) == nbgpu.NBG_EINVAL
+    assert L.nbg_sqr(None, a.ctypes.data, 2) == nbgpu.NBG_EINVAL
+    assert L.nbg_mul(a.ctypes.data, a.ctypes.data, 2, r.ctypes.data, 1) == nbgpu.NBG_EINVAL
+    assert b"alias" in L.nbg_last_error()
+    N = ctypes.c_int64()
+    assert L.nbg_ntt_len(0, ctypes.byref(N)) == nbgpu.NBG_EINVAL
+    assert L.nbg_ntt_len((315 << 34) + 1, ctypes.byref(N)) == nbgpu.NBG_ERANGE
+    assert L.nbg_last_error()
+
+
+def test_tuning_round_trip():
+    old = nbgpu.get_tuning()
+    try:
+        nbgpu.set_tuning('{"last_max": 2048, "cmax": 64}')
+        t = nbgpu.get_tuning()
+        assert '"last_max": 2048' in t and '"cmax": 64' in t
+        with pytest.raises(nbgpu.NBGError):
+            nbgpu.set_tuning('{"cmax": 3}')
+    finally:
+        nbgpu.set_tuning(old)
+    assert nbgpu.get_tuning() == old
+
+
+def test_dispatch_thresholds():
+    # mul! admits the NTT at n >= 64 and m + n >= 304 (src/mul.jl:388); sqr! at n >= 160 (:146)
+    assert nbgpu.uses_fpntt_mul(152, 152) and not nbgpu.uses_fpntt_mul(151, 152)
+    assert nbgpu.uses_fpntt_mul(1000, 64) and not nbgpu.uses_fpntt_mul(1000, 63)
+    assert nbgpu.uses_fpntt_sqr(160) and not nbgpu.uses_fpntt_sqr(159)
+
+
+# ---------------------------------------------------------------------------
+# Index arithmetic of the pass kernels, emulated on the CPU: every tile's loads
+# stay inside [0, N), each pass covers every element exactly once, and every
+# butterfly a tile runs is the reference's butterfly (same global lanes, same
+# twiddle column) for its stage (fp_stage!, src/fpntt.jl:703-713).
+
+def _emulate_plan(N, layout):
+    stages, passes = layout["stages"], layout["passes"]
+    covered_stage = {s: 0 for s in range(len(stages))}
+    for (sa, sb, G, C, Qb, ntiles) in passes:
+        assert C & (C - 1) == 0 and Qb % C == 0 and G * C <= 8192
+        La = stages[sa][1]
+        assert La % Qb == 0 and La // Qb == G
+        per = Qb // C
+        t = np.arange(ntiles, dtype=np.int64)
+        blk, jc = t // per, t % per
+        j0 = jc * C
+        base = blk * La + j0
+        k = np.arange(G, dtype=np.int64)[:, None]
+        c = np.arange(C, dtype=np.int64)[None, :]
+        idx = base[:, None, None] + c[None] + k[None] * Qb  # (tile, k, c)
+        flat = idx.ravel()
+        assert flat.min() >= 0 and flat.max() < N
+        assert np.array_equal(np.sort(flat), np.arange(N))
+        lc = C.bit_length() - 1
+        for s in range(sa, sb + 1):
+            m, Ls, Qs = stages[s]
+            Lloc, Qloc = Ls // Qb, Qs // Qb
+            nb = (G // m) * C
+            e = np.arange(nb, dtype=np.int64)
+            cc, row = e & (C - 1), e >> lc
+            blk_l, jl = row // Qloc, row % Qloc
+            lbase = ((blk_l * Lloc + jl) << lc) + cc
+            stride = Qloc << lc
+            jt = jl[None, :] * Qb + j0[:, None] + cc[None, :]  # twiddle column per tile
+            assert jt.min() >= 0 and jt.max() < Qs
+            lanes = []
+            for tl in range(m):
+                l = lbase + tl * stride
+                assert l.max() < G * C
+                kk, c2 = l >> lc, l & (C - 1)
+                lanes.append(base[:, None] + c2[None, :] + kk[None, :] * Qb)
+            g0 = lanes[0]
+            # reference butterfly: lanes at o + j + t*Q_s with j = g0 mod L_s, j < Q_s
+            assert np.array_equal(g0 % Ls, jt)
+            for tl in range(1, m):
+                assert np.array_equal(lanes[tl], g0 + tl * Qs)
+            covered_stage[s] += g0.size
+        for s in range(sa, sb + 1):
+            assert covered_stage[s] == N // stages[s][0]
+    assert [st for st in covered_stage.values()] == [N // s[0] for s in stages]
+    assert passes[-1][4] == 1 and passes[-1][1] == len(stages) - 1
+
+
+EMU_N = (4, 8, 12, 48, 240, 420, 1260, 4032, 960, 1680, 12288, 20480, 7 * 2**15, 9 * 2**11, 105 * 2**11,
+         2**16, 315 * 2**10, 63 * 2**12, 45 * 2**11, 2**17 * 3)
+EMU_TUNINGS = (None,
+               '{"full_max_mul": 4, "full_max_sqr": 4, "last_max": 4, "early_gmax": 2, "tile_target": 8, "cmax": 2}',
+               '{"full_max_mul": 16, "full_max_sqr": 16, "last_max": 64, "early_gmax": 16, "tile_target": 64, "cmax": 8}',
+               '{"full_max_mul": 256, "full_max_sqr": 256, "last_max": 256, "early_gmax": 64, "tile_target": 512, "cmax": 32}')
+
+
+@pytest.mark.parametrize("tun", EMU_TUNINGS)
+def test_pass_index_emulation(tun):
+    old = nbgpu.get_tuning()
+    try:
+        if tun:
+            nbgpu.set_tuning(tun)
+        for N in EMU_N:
+            for sqr in (False, True):
+                _emulate_plan(N, nbgpu.plan_layout(N, sqr))
+    finally:
+        nbgpu.set_tuning(old)
+
+
+def test_large_plan_layouts():
+    for N in (7 * 2**19, 7 * 2**23, 315 * 2**14, 315 * 2**17, 2**26):
+        lay = nbgpu.plan_layout(N)
+        assert 2 <= len(lay["passes"]) <= 6
+        for (sa, sb, G, C, Qb, nt) in lay["passes"]:
+            assert G * C * 8 * 2 <= 227 * 1024
+    _emulate_plan(315 * 2**14, nbgpu.plan_layout(315 * 2**14))
+
+
+def test_unpack_tile_coefficient_ranges():
+    # k_unpack: coefficients overlapping limbs [w0-1, w0+1024) fit its shared
+    # memory and index x[(N - i) mod N] inside [0, N)
+    TL = 1024
+    for bits, b in ((64 * 4096, 43), (64 * 2**16, 41), (64, 49), (64 * 5, 48), (64 * 2**20, 39)):
+        nconv = 2 * (-(-bits // b)) - 1
+        rn = 2 * (-(-bits // 64))
+        N = nbgpu.ntt_len(nconv)
+        ncoef_cap = (64 * (TL + 2) + 100) // b + 4
+        for tile in range(-(-rn // TL)):
+            w0, w1 = tile * TL, min(tile * TL + TL, rn)
+            wlo = max(w0 - 1, 0)
+            a = 64 * wlo - 99
+            ilo = 0 if a <= 0 else -(-a // b)
+            ihi = min((64 * (w1 - 1) + 63) // b, nconv - 1)
+            assert ihi - ilo + 1 <= ncoef_cap
+            assert 0 <= ilo and ihi < N
+            for w in (wlo, w1 - 1):
+                lo_i = max(0, -(-(64 * w - 99) // b))
+                hi_i = (64 * w + 63) // b
+                assert lo_i >= ilo and min(hi_i, nconv - 1) <= ihi

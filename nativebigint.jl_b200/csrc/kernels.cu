@@ -493,9 +493,14 @@ cudaError_t kernels_init(double p1, double p2) {
     cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const void* ks[] = {(const void*)k_fwd, (const void*)k_pwr, (const void*)k_rev, (const void*)k_unpack};
     for (const void* k : ks) {
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, g_smem_optin);
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, k);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 g_smem_optin - (int)fa.sharedSizeBytes);
         if (e != cudaSuccess) return e;
     }
+    g_smem_optin -= 4096;  // headroom for the largest static allocation (k_unpack)
     return cudaSuccess;
 }
 

@@ -159,7 +159,9 @@ def test_unpack_long_carry_chains(gpu_lib):
     k = total_bits // 64 - 2
     T = (1 << (64 * k)) - 1
     d = [(T >> (b * i)) & ((1 << b) - 1) for i in range(nconv)]
-    e = [int(rng.integers(0, 2**40)) for _ in range(nconv - 1)] + [0]
+    # digits below 64k/b are all-ones (>= 2^40), so any borrow e_(i-1) < 2^40 keeps c_i >= 0
+    full = (64 * k) // b
+    e = [int(rng.integers(0, 2**40)) if i < full - 1 else 0 for i in range(nconv)]
     cs = [d[i] + (e[i] << b) - (e[i - 1] if i else 0) for i in range(nconv)]
     assert all(0 <= c < O.P1 * O.P2 for c in cs)
     x1, x2 = _unpack_case(rng, b, cs, N)

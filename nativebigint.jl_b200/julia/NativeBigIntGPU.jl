@@ -1,0 +1,87 @@
+# NativeBigIntGPU.jl — Julia binding of libnbgpu.so for NativeBigInt.jl.
+#
+# Drop-in for the fp-NTT branch of the reference's mpn multiply: the engine
+# functions mul_fpntt2!/sqr_fpntt2! (src/fpntt.jl:982, :1016) keep their
+# signatures and call the B200 engine through ccall.  Results are bit-identical
+# to the CPU engine.  Karatsuba and basecase products stay on the CPU.
+#
+# Usage (inside NativeBigInt, after `include("fpntt.jl")`):
+#     include("NativeBigIntGPU.jl"); using .NativeBigIntGPU
+#     NativeBigIntGPU.install!()     # route mul_fpntt2!/sqr_fpntt2! to the GPU
+module NativeBigIntGPU
+
+const Limb = UInt64
+const LIB = get(ENV, "NBGPU_LIB", joinpath(@__DIR__, "..", "lib", "libnbgpu.so"))
+
+const NBG_ERANGE = Cint(2)
+
+struct NBGError <: Exception
+    code::Cint
+    msg::String
+end
+Base.showerror(io::IO, e::NBGError) = print(io, "nbgpu error ", e.code, ": ", e.msg)
+
+function check(rc::Cint)
+    rc == 0 && return nothing
+    msg = unsafe_string(ccall((:nbg_last_error, LIB), Cstring, ()))
+    # the reference throws ArgumentError past 315*2^34 points (src/fpntt.jl:948-949)
+    rc == NBG_ERANGE && throw(ArgumentError(msg))
+    throw(NBGError(rc, msg))
+end
+
+# r[ro+1 .. ro+m+n] = a[ao+1 .. ao+m] * b[bo+1 .. bo+n]   (mul_fpntt2!, src/fpntt.jl:982)
+function gpu_mul_fpntt2!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, m::Int,
+                         b::Memory{Limb}, bo::Int, n::Int)
+    @boundscheck (ro + m + n <= length(r) && ao + m <= length(a) && bo + n <= length(b)) ||
+        throw(BoundsError())
+    GC.@preserve r a b begin
+        rc = ccall((:nbg_mul, LIB), Cint,
+                   (Ptr{Limb}, Ptr{Limb}, Int64, Ptr{Limb}, Int64),
+                   pointer(r, ro + 1), pointer(a, ao + 1), m, pointer(b, bo + 1), n)
+    end
+    check(rc)
+    return nothing
+end
+
+# r[ro+1 .. ro+2n] = a[ao+1 .. ao+n]^2   (sqr_fpntt2!, src/fpntt.jl:1016)
+function gpu_sqr_fpntt2!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, n::Int)
+    @boundscheck (ro + 2n <= length(r) && ao + n <= length(a)) || throw(BoundsError())
+    GC.@preserve r a begin
+        rc = ccall((:nbg_sqr, LIB), Cint, (Ptr{Limb}, Ptr{Limb}, Int64),
+                   pointer(r, ro + 1), pointer(a, ao + 1), n)
+    end
+    check(rc)
+    return nothing
+end
+
+# Batched products: descs as in include/nbgpu.h (nbg_desc); b == C_NULL squares a.
+struct NbgDesc
+    r::Ptr{Limb}
+    a::Ptr{Limb}
+    b::Ptr{Limb}
+    m::Int64
+    n::Int64
+    bits_a::Int64
+    bits_b::Int64
+end
+
+function gpu_mul_batch!(descs::Vector{NbgDesc})
+    rc = ccall((:nbg_mul_batch, LIB), Cint, (Ptr{NbgDesc}, Int64), descs, length(descs))
+    check(rc)
+    return nothing
+end
+
+# Replaces the engine entry points of the enclosing NativeBigInt module so every
+# NTT-sized mul!/sqr!/mul_bal! (src/mul.jl:134, :146, :161, :388-390) and NBig *
+# (src/nbig.jl:124-140) run on the GPU.
+function install!(mod::Module = parentmodule(@__MODULE__))
+    @eval mod begin
+        mul_fpntt2!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, m::Int, b::Memory{Limb}, bo::Int, n::Int) =
+            $(gpu_mul_fpntt2!)(r, ro, a, ao, m, b, bo, n)
+        sqr_fpntt2!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, n::Int) =
+            $(gpu_sqr_fpntt2!)(r, ro, a, ao, n)
+    end
+    return nothing
+end
+
+end # module

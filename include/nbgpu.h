@@ -44,6 +44,23 @@ int nbg_sqr(uint64_t *r, const uint64_t *a, int64_t n);
 int nbg_mul_dev(uint64_t *r, const uint64_t *a, int64_t m, const uint64_t *b, int64_t n, void *stream);
 int nbg_sqr_dev(uint64_t *r, const uint64_t *a, int64_t n, void *stream);
 
+/* No counterpart in the reference (Julia allocates freely).  The same product
+ * as nbg_mul_dev (device buffers, b == NULL for a square, asynchronous on
+ * `stream` after reading the two top limbs), for callers that cannot allocate
+ * GPU memory: code running inside a memory arena or pool that owns the whole
+ * device, under an allocator hook that must not recurse, or in a foreign
+ * runtime that lends only the input and output buffers.  It calls no
+ * cudaMalloc/cudaFree and no allocating library routine; its workspace is a
+ * fixed 16 MiB device array inside the library (held on every GPU that loads
+ * the library until exit), located once per device with cudaGetSymbolAddress
+ * on the first call there — make that first call before any stream capture.
+ * Products that do not fit return NBG_ENOMEM: transform lengths above about
+ * 3.4e5 points for products (balanced operands above about 2^16 limbs) or
+ * 5.2e5 points for squares.  All calls
+ * share the array: calls that overlap on the GPU race; order them on one
+ * stream. */
+int nbg_mul_dev_noalloc(uint64_t *r, const uint64_t *a, int64_t m, const uint64_t *b, int64_t n, void *stream);
+
 /* ---- batches ------------------------------------------------------------- */
 
 /* One product of a batch.  b == NULL (or b == a with n == m) requests the

@@ -35,6 +35,7 @@ EXPORTS = [
     "nbg_ntt_params", "nbg_ntt_len", "nbg_magnitude_bits", "nbg_pack_dev", "nbg_ntt_fwd_dev",
     "nbg_ntt_rev_dev", "nbg_pointwise_dev", "nbg_unpack_dev", "nbg_plan_info", "nbg_plan_layout", "nbg_set_tuning",
     "nbg_get_tuning", "nbg_init", "nbg_last_error", "nbg_default_stream", "nbg_launch_count",
+    "nbg_mul_dev_noalloc",
 ]
 
 
@@ -70,6 +71,7 @@ def lib() -> ctypes.CDLL:
             "nbg_sqr": [vp, vp, i64],
             "nbg_mul_dev": [vp, vp, i64, vp, i64, vp],
             "nbg_sqr_dev": [vp, vp, i64, vp],
+            "nbg_mul_dev_noalloc": [vp, vp, i64, vp, i64, vp],
             "nbg_mul_batch": [vp, i64],
             "nbg_mul_batch_dev": [vp, i64, vp],
             "nbg_batch_create": [vp, i64, c.POINTER(vp)],
@@ -210,6 +212,12 @@ def mul_dev(r, a, m: int, b, n: int, stream=None) -> None:
 
 def sqr_dev(r, a, n: int, stream=None) -> None:
     _check(lib().nbg_sqr_dev(_dptr(r), _dptr(a), n, _stream(stream)))
+
+
+def mul_dev_noalloc(r, a, m: int, b, n: int, stream=None) -> None:
+    """The product of nbg_mul_dev with no device allocation: the workspace is the
+    library's fixed 16 MiB device array (b None for a square)."""
+    _check(lib().nbg_mul_dev_noalloc(_dptr(r), _dptr(a), m, None if b is None else _dptr(b), n, _stream(stream)))
 
 
 def make_descs(items) -> ctypes.Array:

@@ -352,13 +352,14 @@ def run_ours(args, rank: int, world: int) -> None:
         # unbatched: the same products one call each (device buffers)
         lat = []
         nb = min(args.unbatched, count)
+        unbatched = None
         one = (nbgpu.NbgDesc * 1)()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ul = 0
-        for k in range(nb):
+        for k in range(nb if nb > 0 else 0):
             one[0] = descs[k]
             c0 = time.perf_counter()
             nbgpu.mul_batch_dev(one, s)
@@ -366,9 +367,10 @@ def run_ours(args, rank: int, world: int) -> None:
             ul += int(W["m"][k] + W["n"][k])
         torch.cuda.synchronize()
         un_s = time.perf_counter() - t0
-        unbatched = {"value": ul / un_s, "unit": "output limbs/s", "products": nb,
-                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                     "products_per_s": nb / un_s}
+        if nb > 0:
+            unbatched = {"value": ul / un_s, "unit": "output limbs/s", "products": nb,
+                         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                         "products_per_s": nb / un_s}
 
         # e2e: host buffers through nbg_mul_batch (pinned), copies inside the call
         pin_in = torch.from_numpy(limbs).pin_memory()
@@ -394,8 +396,12 @@ def run_ours(args, rank: int, world: int) -> None:
 
         # CPU baseline on a bounded sample
         threads = os.cpu_count() or 1
-        idx, desc = cpu_sample(W, args.cpu_seconds, threads)
-        cpu_v, _ = cpu_rate(W, idx, threads)
+        cpu_base = None
+        if args.cpu_seconds > 0:
+            idx, desc = cpu_sample(W, args.cpu_seconds, threads)
+            cpu_v, _ = cpu_rate(W, idx, threads)
+            cpu_base = {"value": cpu_v, "unit": "output limbs/s", "cores": threads, "kind": "port",
+                        "sample": desc + "; CPU restatement of src/fpntt.jl (Julia is not installed)"}
 
         clocks = clk.summary()
         med = statistics.median(step_ms)
@@ -408,7 +414,7 @@ def run_ours(args, rank: int, world: int) -> None:
                        "parallelism": f"batch shards x{world}, no collective"},
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
             "products_per_s": count * world / (total_ms_max / args.steps / 1e3),
-            "vs_unbatched": value / world / unbatched["value"],
+            "vs_unbatched": value / world / unbatched["value"] if unbatched else None,
             "unbatched": unbatched,
             "bitexact": {"checked_vs_gmp": int(len(chk)), "mismatches": bad},
             "e2e": {"value": e2e_val, "unit": "output limbs/s",
@@ -416,8 +422,7 @@ def run_ours(args, rank: int, world: int) -> None:
             "gpu_launches": int(launches),
             "clocks": clocks,
             "roofline": roof,
-            "cpu_baseline": {"value": cpu_v, "unit": "output limbs/s", "cores": threads, "kind": "port",
-                             "sample": desc + "; CPU restatement of src/fpntt.jl (Julia is not installed)"},
+            "cpu_baseline": cpu_base,
             "median_step_ms": med,
         }
         print(json.dumps(line), flush=True)

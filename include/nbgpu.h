@@ -136,10 +136,11 @@ int nbg_unpack_dev(uint64_t *r, int64_t rn, const double *x1, const double *x2, 
 int nbg_plan_info(int64_t N, int32_t *nst, int32_t *npass, int32_t *stage_m, int32_t *pass_end, int32_t cap);
 /* Host-only view of the plan for length N under the current tuning (no
  * device needed): stages[3*i..] = (radix, span L, stride Q) in forward order,
- * passes[6*j..] = (first stage, last stage, rows G, columns C, column stride
- * Qb, tiles).  `cap` bounds both arrays' entry counts (stages and passes). */
+ * passes[7*j..] = (first stage, last stage, rows G, columns C, column stride
+ * Qb, tiles, rounds), rounds[j*cap + r] = (round kind << 8) | first stage
+ * (rounds may be NULL).  `cap` bounds the entry counts. */
 int nbg_plan_layout(int64_t N, int32_t sqr, int64_t *stages, int32_t *nst, int64_t *passes, int32_t *npass,
-                    int32_t cap);
+                    int32_t *rounds, int32_t cap);
 /* Tuning knobs (JSON object, keys: full_max_mul, full_max_sqr, last_max,
  * early_gmax, tile_target, cmax).  Changing them drops cached plans. */
 int nbg_set_tuning(const char *json);

@@ -210,13 +210,13 @@ int transform_passes(double* x, int64_t N, int prime, bool fwd, cudaStream_t st)
     PlanRec* pr;
     int rc = E.get_plan(N, 0, &pr);
     if (rc) return rc;
+    // the pass kernels transform both primes' tiles together: the other prime
+    // works on a scratch copy in the pool that is discarded
     DProd P;
     memset(&P, 0, sizeof P);
     P.plan = pr->slot;
     P.npass = pr->d.npass;
     P.flags = PF_PRELOADED;
-    P.xa[prime] = x;
-    P.xa[1 - prime] = x;
     std::vector<Job> jobs;
     std::vector<Launch> ls;
     const int np = pr->d.npass;
@@ -224,14 +224,17 @@ int transform_passes(double* x, int64_t N, int prime, bool fwd, cudaStream_t st)
         const int p = fwd ? i : np - 1 - i;
         const DPass& ps = pr->d.pass[p];
         Launch L{fwd ? (int)JK_FWD : (int)JK_REV, (int64_t)jobs.size(), ps.ntiles,
-                 sizeof(double) * (size_t)ps.G * (size_t)ps.C};
-        for (int64_t t = 0; t < ps.ntiles; t++) jobs.push_back(Job{0, prime | (p << 8), t});
+                 sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C)};
+        for (int64_t t = 0; t < ps.ntiles; t++) jobs.push_back(Job{0, p << 8, t});
         ls.push_back(L);
     }
     const size_t jo = 256;
-    rc = E.ensure_pool(jo + sizeof(Job) * jobs.size());
+    const size_t so = align_up(jo + sizeof(Job) * jobs.size(), 256);
+    rc = E.ensure_pool(so + sizeof(double) * (size_t)N);
     if (rc) return rc;
     char* d = (char*)E.pool;
+    P.xa[prime] = x;
+    P.xa[1 - prime] = (double*)(d + so);
     CUDA_TRY(cudaMemcpyAsync(d, &P, sizeof P, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(d + jo, jobs.data(), sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, st));
     for (const Launch& L : ls) {
@@ -540,7 +543,7 @@ int nbg_plan_info(int64_t N, int32_t* nst, int32_t* npass, int32_t* stage_m, int
 }
 
 int nbg_plan_layout(int64_t N, int32_t sqr, int64_t* stages, int32_t* nst, int64_t* passes, int32_t* npass,
-                    int32_t cap) {
+                    int32_t* rounds, int32_t cap) {
     if (!stages || !nst || !passes || !npass || cap < 1) return fail(NBG_EINVAL, "bad argument");
     API_LOCK();
     DPlan d;
@@ -554,8 +557,10 @@ int nbg_plan_layout(int64_t N, int32_t sqr, int64_t* stages, int32_t* nst, int64
     }
     for (int j = 0; j < d.npass; j++) {
         const DPass& p = d.pass[j];
-        int64_t* o = passes + 6 * j;
-        o[0] = p.sa; o[1] = p.sb; o[2] = p.G; o[3] = p.C; o[4] = p.Qb; o[5] = p.ntiles;
+        int64_t* o = passes + 7 * j;
+        o[0] = p.sa; o[1] = p.sb; o[2] = p.G; o[3] = p.C; o[4] = p.Qb; o[5] = p.ntiles; o[6] = p.nrounds;
+        if (rounds)
+            for (int r = 0; r < p.nrounds && r < cap; r++) rounds[j * cap + r] = (p.rkind[r] << 8) | p.rstage[r];
     }
     *nst = d.nst;
     *npass = d.npass;

@@ -201,9 +201,9 @@ static int64_t pow2floor(int64_t x) {
 std::string Tuning::to_json() const {
     char buf[256];
     snprintf(buf, sizeof buf,
-             "{\"full_max_mul\": %d, \"full_max_sqr\": %d, \"last_max\": %d, \"early_gmax\": %d, "
-             "\"tile_target\": %d, \"cmax\": %d}",
-             full_max_mul, full_max_sqr, last_max, early_gmax, tile_target, cmax);
+             "{\"full_max_mul\": %d, \"full_max_sqr\": %d, \"last_max\": %d, \"last_max_sqr\": %d, "
+             "\"early_gmax\": %d, \"tile_target\": %d, \"cmax\": %d}",
+             full_max_mul, full_max_sqr, last_max, last_max_sqr, early_gmax, tile_target, cmax);
     return buf;
 }
 
@@ -225,13 +225,16 @@ int Tuning::from_json(const char* js) {
     json_int(js, "full_max_mul", &t.full_max_mul);
     json_int(js, "full_max_sqr", &t.full_max_sqr);
     json_int(js, "last_max", &t.last_max);
+    json_int(js, "last_max_sqr", &t.last_max_sqr);
     json_int(js, "early_gmax", &t.early_gmax);
     json_int(js, "tile_target", &t.tile_target);
     json_int(js, "cmax", &t.cmax);
     auto pow2 = [](int v) { return v >= 1 && (v & (v - 1)) == 0; };
-    if (!pow2(t.cmax) || t.last_max < 4 || t.early_gmax < 2 || t.tile_target < 1 || t.full_max_mul < 4 ||
-        t.full_max_sqr < 4 || t.full_max_mul > 8192 || t.full_max_sqr > 16384 || t.last_max > 8192 ||
-        t.early_gmax > 4096 || t.tile_target > 8192)
+    // shared memory bounds: a product's last pass holds 4 tiles (a, b per
+    // prime), a square's 2; column passes hold 2 tiles of <= tile_target or G.
+    if (!pow2(t.cmax) || t.last_max < 4 || t.last_max_sqr < 4 || t.early_gmax < 2 || t.tile_target < 1 ||
+        t.full_max_mul < 4 || t.full_max_sqr < 4 || t.full_max_mul > 4096 || t.full_max_sqr > 8192 ||
+        t.last_max > 4096 || t.last_max_sqr > 8192 || t.early_gmax > 1024 || t.tile_target > 8192)
         return fail(NBG_EINVAL, "tuning out of range");
     *this = t;
     return NBG_OK;
@@ -280,7 +283,8 @@ int plan_structure(int64_t N, int for_sqr, const Tuning& tun, DPlan& d) {
     for (int64_t v : okm) okm_hit |= (m == v);
     if (!okm_hit || !(m == 1 || k >= 2) || k > std::min(TWOADIC[0], TWOADIC[1]))
         return fail(NBG_EINVAL, "inadmissible transform length %lld", (long long)N);
-    if (N > (int64_t(1) << 33)) return fail(NBG_ENOMEM, "transform length %lld too large for one GPU", (long long)N);
+    // device indices are 32-bit: 2^31 points is a 16 GB transform buffer
+    if (N >= (int64_t(1) << 31)) return fail(NBG_ENOMEM, "transform length %lld too large for one GPU", (long long)N);
 
     memset(&d, 0, sizeof d);
     d.N = N;
@@ -330,11 +334,12 @@ int plan_structure(int64_t N, int for_sqr, const Tuning& tun, DPlan& d) {
     // last_max (a contiguous block, C = 1); earlier stages are grouped
     // greedily into column passes of at most early_gmax rows.
     const int full_max = for_sqr ? tun.full_max_sqr : tun.full_max_mul;
+    const int last_max = for_sqr ? tun.last_max_sqr : tun.last_max;
     int a = 0;
     if (N > full_max) {
         a = S - 1;
         for (int s = 0; s < S; s++)
-            if (hs[s].L <= tun.last_max) { a = s; break; }
+            if (hs[s].L <= last_max) { a = s; break; }
         if (a == 0) a = 1;
     }
     int np = 0;
@@ -366,6 +371,46 @@ int plan_structure(int64_t N, int for_sqr, const Tuning& tun, DPlan& d) {
         ps.ntiles = N / hs[a].L;
     }
     d.npass = np;
+    // rounds: odd stages one by one; the pass's radix-4 run is paired from its
+    // smallest span upwards (radix-8 round for the span-8 stage and radix-2
+    // when the transform ends with one), a leftover radix-4 at the top alone.
+    for (int p = 0; p < np; p++) {
+        DPass& ps = d.pass[p];
+        int nr = 0;
+        int s = ps.sa;
+        for (; s <= ps.sb && (hs[s].m == 3 || hs[s].m == 5 || hs[s].m == 7); s++) {
+            ps.rkind[nr] = RK_ODD;
+            ps.rstage[nr++] = (int8_t)s;
+        }
+        int8_t kind[MAXST], first[MAXST];
+        int nb = 0;
+        int e = ps.sb;
+        if (e >= s && hs[e].m == 2) {
+            if (e - 1 >= s && hs[e - 1].m == 4 && hs[e - 1].L == 8) {
+                kind[nb] = RK_R8;
+                first[nb++] = (int8_t)(e - 1);
+                e -= 2;
+            } else {
+                kind[nb] = RK_R2;
+                first[nb++] = (int8_t)e;
+                e -= 1;
+            }
+        }
+        while (e - 1 >= s) {
+            kind[nb] = RK_R16;
+            first[nb++] = (int8_t)(e - 1);
+            e -= 2;
+        }
+        if (e == s) {
+            kind[nb] = RK_R4;
+            first[nb++] = (int8_t)s;
+        }
+        for (int i = nb - 1; i >= 0; i--) {
+            ps.rkind[nr] = kind[i];
+            ps.rstage[nr++] = first[i];
+        }
+        ps.nrounds = nr;
+    }
     return NBG_OK;
 }
 
@@ -550,27 +595,27 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
     bb.xb_off = xb_off;
     bb.agg_off = agg_off;
 
-    // jobs per step (alignment: every product's pointwise pass runs in one launch)
     std::vector<std::vector<Job>> fwd((size_t)std::max(pmax - 1, 0)), rev((size_t)std::max(pmax - 1, 0));
     std::vector<Job> pwr, unp, car;
     std::vector<size_t> fwd_smem(fwd.size(), 0), rev_smem(rev.size(), 0);
     size_t pwr_smem = 0;
+
     // algorithmic FP64 instructions per butterfly of the reference schedule
     // (fwd, rev), counted on the oracle's restatement: radix-2 10, radix-3 32,
     // radix-4 40, radix-5 94/98, radix-7 173/201; pointwise 7 per point; the
     // Garner unpack 28 per coefficient.
-    auto bfly_ops = [](int m, bool fwd) -> double {
+    auto bfly_ops = [](int m, bool fwd_dir) -> double {
         switch (m) {
             case 2: return 10;
             case 3: return 32;
             case 4: return 40;
-            case 5: return fwd ? 94 : 98;
-            default: return fwd ? 173 : 201;
+            case 5: return fwd_dir ? 94 : 98;
+            default: return fwd_dir ? 173 : 201;
         }
     };
-    auto pass_ops = [&](const DPlan& pl, const DPass& ps, bool fwd) {
+    auto pass_ops = [&](const DPlan& pl, const DPass& ps, bool fwd_dir) {
         double o = 0;
-        for (int s = ps.sa; s <= ps.sb; s++) o += bfly_ops(pl.st[s].m, fwd) * (double)ps.G * ps.C / pl.st[s].m;
+        for (int s = ps.sa; s <= ps.sb; s++) o += bfly_ops(pl.st[s].m, fwd_dir) * (double)ps.G * ps.C / pl.st[s].m;
         return o;
     };
     std::vector<double> fwd_ops(fwd.size(), 0), fwd_bytes(fwd.size(), 0), rev_ops(fwd.size(), 0),
@@ -586,27 +631,29 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
             const DPass& ps = pl.pass[p];
             const size_t step = (size_t)(pmax - Pn + p);
             fwd_ops[step] += 2.0 * ops_cnt * pass_ops(pl, ps, true) * (double)ps.ntiles;
-            const double in_b = p == 0 ? (double)(P.nca + (P.sqr ? 0 : P.ncb)) * P.bch / 8.0 * 2.0
+            const double in_b = p == 0 ? (double)(P.nca + (P.sqr ? 0 : P.ncb)) * P.bch / 8.0
                                        : 2.0 * ops_cnt * 8.0 * N;
             fwd_bytes[step] += in_b + 2.0 * ops_cnt * 8.0 * N;
         }
         {
             const DPass& ps = pl.pass[Pn - 1];
-            pwr_ops += 2.0 * (ops_cnt * pass_ops(pl, ps, true) + 7.0 * ps.G + pass_ops(pl, ps, false)) * (double)ps.ntiles;
-            const double in_b = Pn == 1 ? (double)(P.nca + (P.sqr ? 0 : P.ncb)) * P.bch / 8.0 * 2.0
+            pwr_ops += 2.0 * (ops_cnt * pass_ops(pl, ps, true) + 7.0 * ps.G + pass_ops(pl, ps, false)) *
+                       (double)ps.ntiles;
+            const double in_b = Pn == 1 ? (double)(P.nca + (P.sqr ? 0 : P.ncb)) * P.bch / 8.0
                                         : 2.0 * ops_cnt * 8.0 * N;
             pwr_bytes += in_b + 2.0 * 8.0 * N;
         }
         for (int p = Pn - 2; p >= 0; p--) {
-            const DPass& ps = pl.pass[p];
             const size_t step = (size_t)(Pn - 2 - p);
-            rev_ops[step] += 2.0 * pass_ops(pl, ps, false) * (double)ps.ntiles;
+            rev_ops[step] += 2.0 * pass_ops(pl, pl.pass[p], false) * (double)pl.pass[p].ntiles;
             rev_bytes[step] += 2.0 * 16.0 * N;
         }
         unp_ops += 28.0 * (double)P.nconv;
         unp_bytes += 16.0 * (double)P.nconv + 8.0 * (double)P.rn;
     }
 
+    // jobs per step (alignment: every product's pointwise pass runs in one launch);
+    // each pass job covers one tile of both primes
     for (int64_t k = 0; k < count; k++) {
         const DProd& P = bb.prods[(size_t)k];
         const DPlan& pl = bb.plan_of[(size_t)k]->d;
@@ -614,24 +661,20 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         for (int p = 0; p < Pn - 1; p++) {
             const DPass& ps = pl.pass[p];
             const size_t step = (size_t)(pmax - Pn + p);
-            for (int f = 0; f < 2; f++)
-                for (int op = 0; op < (P.sqr ? 1 : 2); op++)
-                    for (int64_t t = 0; t < ps.ntiles; t++)
-                        fwd[step].push_back(Job{(int32_t)k, f | (op << 1) | (p << 8), t});
-            fwd_smem[step] = std::max(fwd_smem[step], sizeof(double) * (size_t)ps.G * (size_t)ps.C);
+            for (int op = 0; op < (P.sqr ? 1 : 2); op++)
+                for (int64_t t = 0; t < ps.ntiles; t++) fwd[step].push_back(Job{(int32_t)k, (op << 1) | (p << 8), t});
+            fwd_smem[step] = std::max(fwd_smem[step], sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C));
         }
         {
             const DPass& ps = pl.pass[Pn - 1];
-            for (int f = 0; f < 2; f++)
-                for (int64_t t = 0; t < ps.ntiles; t++) pwr.push_back(Job{(int32_t)k, f | ((Pn - 1) << 8), t});
-            pwr_smem = std::max(pwr_smem, sizeof(double) * (size_t)ps.G * (size_t)ps.C * (P.sqr ? 1 : 2));
+            for (int64_t t = 0; t < ps.ntiles; t++) pwr.push_back(Job{(int32_t)k, (Pn - 1) << 8, t});
+            pwr_smem = std::max(pwr_smem, sizeof(double) * (P.sqr ? 2 : 4) * (size_t)tile_stride_doubles(ps.G * ps.C));
         }
         for (int p = Pn - 2; p >= 0; p--) {
             const DPass& ps = pl.pass[p];
             const size_t step = (size_t)(Pn - 2 - p);
-            for (int f = 0; f < 2; f++)
-                for (int64_t t = 0; t < ps.ntiles; t++) rev[step].push_back(Job{(int32_t)k, f | (p << 8), t});
-            rev_smem[step] = std::max(rev_smem[step], sizeof(double) * (size_t)ps.G * (size_t)ps.C);
+            for (int64_t t = 0; t < ps.ntiles; t++) rev[step].push_back(Job{(int32_t)k, p << 8, t});
+            rev_smem[step] = std::max(rev_smem[step], sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C));
         }
         for (int64_t t = 0; t < P.ntl; t++) unp.push_back(Job{(int32_t)k, 0, t});
         if (P.ntl > 1) car.push_back(Job{(int32_t)k, 0, 0});

@@ -23,9 +23,10 @@ int ntt_params(int64_t bits_a, int64_t bits_b, int* b_out, int64_t* N_out);
 
 // Pass-split knobs (the autotuner's search space).
 struct Tuning {
-    int full_max_mul = 4096;  // one-pass (whole transform in shared memory) up to this N, products
-    int full_max_sqr = 8192;  // same for squares (one operand tile)
-    int last_max = 4096;      // largest contiguous block of the last pass
+    int full_max_mul = 2048;  // one-pass (whole transform in shared memory) up to this N, products
+    int full_max_sqr = 4096;  // same for squares (one operand tile per prime)
+    int last_max = 2048;      // largest contiguous block of the last pass, products
+    int last_max_sqr = 4096;  // same for squares
     int early_gmax = 256;     // largest row count of an early (column) pass
     int tile_target = 2048;   // target doubles per column-pass tile
     int cmax = 128;           // most adjacent columns per column-pass tile

@@ -1,7 +1,7 @@
 // kernels.cu — the fp-NTT product pipeline on sm_100a FP64 cores.
 //
 // Kernels (each is a work-queue launch: CTA i takes Job i of a host-built list
-// that may mix products of any size):
+// that may mix products of any size; pass kernels hold both primes' tiles):
 //   k_fwd     forward pass of one tile; pass 0 packs limbs into b-bit chunks
 //             on load (fp_ntt_pack!, src/fpntt.jl:744-768)
 //   k_pwr     last pass: forward stages, pointwise product
@@ -14,6 +14,13 @@
 //   k_twiddle expands exact minimal-balanced twiddle tables from two small
 //             power tables (twiddle values are unique residues, so any exact
 //             construction equals fp_twiddles, :173-186)
+//
+// Within a pass the stages run as rounds (types.h RoundKind): radix-16 rounds
+// hold 16 points per work unit in registers and apply two radix-4 stages
+// between one shared-memory load and store; radix-8 rounds do the span-8
+// radix-4 stage and the final radix-2; odd stages run one butterfly per unit.
+// Every butterfly is the reference's butterfly on the reference's inputs, so
+// the grouping changes no bit.
 #include <cuda_runtime.h>
 
 #include "butterfly.cuh"
@@ -26,6 +33,13 @@ __constant__ double c_garner[2];  // g = p1^-1 mod p2 (canonical) and g/p2
 
 __device__ __forceinline__ Fp fpctx(int f) { return c_fp[f]; }
 
+__device__ __forceinline__ int sp(int i) { return tile_pad_index(i); }
+
+// exact double of an integer below 2^52: OR it into 2^52's mantissa, subtract 2^52
+__device__ __forceinline__ double small_u64_to_double(uint64_t c) {
+    return __dsub_rn(__longlong_as_double((long long)(c | 0x4330000000000000ULL)), 4503599627370496.0);
+}
+
 // ---------------------------------------------------------------------------
 // Pack: chunk i of an n-limb operand (fp_ntt_pack!, :744-768).  The
 // reference's fast loop always ORs in the next limb; its high bits are masked
@@ -33,196 +47,374 @@ __device__ __forceinline__ Fp fpctx(int f) { return c_fp[f]; }
 __device__ __forceinline__ double pack_chunk(const uint64_t* __restrict__ limbs, int64_t n, int b, int64_t nch,
                                              int64_t i) {
     if (i >= nch) return 0.0;
-    int64_t bit = i * (int64_t)b;
-    int64_t w = bit >> 6;
-    int sh = (int)(bit & 63);
+    const uint64_t bit = (uint64_t)i * (uint32_t)b;
+    const int64_t w = (int64_t)(bit >> 6);
+    const int sh = (int)(bit & 63);
     uint64_t c = __ldg(limbs + w) >> sh;
     if (sh + b > 64 && w + 1 < n) c |= __ldg(limbs + w + 1) << (64 - sh);
-    return (double)(c & ((1ULL << b) - 1ULL));
+    return small_u64_to_double(c & ((1ULL << b) - 1ULL));
 }
 
 // ---------------------------------------------------------------------------
-// One stage over a shared-memory tile of G rows x C columns (row stride C).
-// Local stage geometry: Lloc = L_s/Qb rows per block, Qloc = Q_s/Qb.
+// Tiles resident in shared memory: `ntiles` tiles of G rows x C columns
+// (padded layout, row stride C), `stride` doubles apart; tile t belongs to
+// prime t >> pshift.  Column c of a tile is global column j0 + c of the pass.
+struct Tiles {
+    double* s;
+    int stride;
+    int ntiles;
+    int pshift;
+    int G;
+    int lc;   // log2 C
+    int Qb;   // pass column stride (global)
+    int j0;   // first global column of the tile
+};
+
+// unit u of a round over all tiles -> (tile, unit within tile)
+__device__ __forceinline__ int split_unit(int u, int per, int& tau) {
+    tau = 0;
+    while (u >= per) {
+        u -= per;
+        tau++;
+    }
+    return u;
+}
+
+// Generic stage: one butterfly per unit, any radix (odd stages, lone radix-4/2).
 template <int M, bool FWD>
-__device__ __forceinline__ void stage_tile(double* __restrict__ s, int G, int lc, int Lloc, int Qloc,
-                                           const double* __restrict__ tw, int64_t Qs, int64_t Qb, int64_t j0,
-                                           const double* rot, Fp F) {
-    const int C = 1 << lc;
-    const int nb = (G / M) << lc;
-    const int stride = Qloc << lc;
-    double r[8];
-#pragma unroll
-    for (int t = 0; t < 8; t++) r[t] = rot[t];
-    for (int e = threadIdx.x; e < nb; e += blockDim.x) {
-        int c = e & (C - 1);
-        int row = e >> lc;
-        int blk = row / Qloc;
-        int jl = row - blk * Qloc;
-        int base = ((blk * Lloc + jl) << lc) + c;
+__device__ void round_gen(const Tiles& T, const DStage& st) {
+    const int C = 1 << T.lc;
+    const int Lloc = (int)(st.L / T.Qb), Qloc = (int)(st.Q / T.Qb);
+    const int Q = (int)st.Q;
+    const int per = (T.G / M) << T.lc;
+    const int total = per * T.ntiles;
+    // row / Qloc = (row >> e) / odd, odd by multiply-high (exact for rows < 2^32 / odd)
+    const int e = __ffs(Qloc) - 1;
+    const unsigned odd = (unsigned)(Qloc >> e);
+    const unsigned mg = odd == 1 ? 0u : 0xFFFFFFFFu / odd + 1u;
+    const int stride = Qloc << T.lc;
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        int tau;
+        const int uu = split_unit(u, per, tau);
+        const int f = tau >> T.pshift;
+        const Fp F = fpctx(f);
+        double* s = T.s + tau * T.stride;
+        const int c = uu & (C - 1);
+        const int row = uu >> T.lc;
+        const unsigned rs = (unsigned)row >> e;
+        const int blk = odd == 1 ? (int)rs : (int)__umulhi(rs, mg);
+        const int jl = row - blk * Qloc;
+        const int base = ((blk * Lloc + jl) << T.lc) + c;
         double y[M];
 #pragma unroll
-        for (int t = 0; t < M; t++) y[t] = s[base + t * stride];
+        for (int t = 0; t < M; t++) y[t] = s[sp(base + t * stride)];
         if constexpr (M == 2) {
             butterfly2(y[0], y[1], F);
         } else {
+            const int j = jl * T.Qb + T.j0 + c;
+            const double* tw = st.tw[f] + j;
             double w[M];
-            int64_t j = (int64_t)jl * Qb + j0 + c;
             w[0] = 0.0;
 #pragma unroll
-            for (int t = 1; t < M; t++) w[t] = __ldg(tw + (int64_t)(t - 1) * Qs + j);
-            butterfly<M, FWD>(y, w, r, F);
+            for (int t = 1; t < M; t++) w[t] = __ldg(tw + (t - 1) * Q);
+            double rot[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) rot[t] = st.rot[f][t];
+            butterfly<M, FWD>(y, w, rot, F);
         }
 #pragma unroll
-        for (int t = 0; t < M; t++) s[base + t * stride] = y[t];
+        for (int t = 0; t < M; t++) s[sp(base + t * stride)] = y[t];
+    }
+}
+
+// Radix-16 round: stages A (span L) and B (span L/4), both radix-4.  Unit
+// (block b, j2 < L/16 rows, column c) holds rows b*L + j2 + t1*L/4 + t2*L/16.
+// Forward: A's butterflies run over t1 for each t2 (column j2 + t2*L/16), then
+// B's over t2 for each t1 (column j2).  Reverse: B then A, transposed.
+template <bool FWD>
+__device__ void round_r16(const Tiles& T, const DStage& A, const DStage& B) {
+    const int C = 1 << T.lc;
+    const int Lloc = (int)(A.L / T.Qb);
+    const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
+    const int QA = (int)A.Q, QB = (int)B.Q;
+    const int per = (T.G >> 4) << T.lc;
+    const int total = per * T.ntiles;
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        int tau;
+        const int uu = split_unit(u, per, tau);
+        const int f = tau >> T.pshift;
+        const Fp F = fpctx(f);
+        const double wi = A.rot[f][0];  // the same 4th root for every radix-4 stage
+        double* s = T.s + tau * T.stride;
+        const int c = uu & (C - 1);
+        const int r = uu >> T.lc;
+        const int b = r >> lq, j2 = r & (q16 - 1);
+        const int row0 = b * Lloc + j2;
+        double v[16];
+#pragma unroll
+        for (int t1 = 0; t1 < 4; t1++)
+#pragma unroll
+            for (int t2 = 0; t2 < 4; t2++) v[t1 * 4 + t2] = s[sp(((row0 + t1 * 4 * q16 + t2 * q16) << T.lc) + c)];
+        const int jB = j2 * T.Qb + T.j0 + c;
+        const double* twB = B.tw[f] + jB;
+        const double* twA = A.tw[f] + jB;  // A's column for t2 is jB + t2*q16*Qb
+        const int stepA = q16 * T.Qb;
+        if (FWD) {
+#pragma unroll
+            for (int t2 = 0; t2 < 4; t2++) {
+                double y[4] = {v[t2], v[4 + t2], v[8 + t2], v[12 + t2]};
+                double w[4] = {0.0, __ldg(twA + t2 * stepA), __ldg(twA + t2 * stepA + QA),
+                               __ldg(twA + t2 * stepA + 2 * QA)};
+                butterfly<4, true>(y, w, &wi, F);
+                v[t2] = y[0]; v[4 + t2] = y[1]; v[8 + t2] = y[2]; v[12 + t2] = y[3];
+            }
+            const double w[4] = {0.0, __ldg(twB), __ldg(twB + QB), __ldg(twB + 2 * QB)};
+#pragma unroll
+            for (int t1 = 0; t1 < 4; t1++) butterfly<4, true>(v + 4 * t1, w, &wi, F);
+        } else {
+            const double w[4] = {0.0, __ldg(twB), __ldg(twB + QB), __ldg(twB + 2 * QB)};
+#pragma unroll
+            for (int t1 = 0; t1 < 4; t1++) butterfly<4, false>(v + 4 * t1, w, &wi, F);
+#pragma unroll
+            for (int t2 = 0; t2 < 4; t2++) {
+                double y[4] = {v[t2], v[4 + t2], v[8 + t2], v[12 + t2]};
+                double wa[4] = {0.0, __ldg(twA + t2 * stepA), __ldg(twA + t2 * stepA + QA),
+                                __ldg(twA + t2 * stepA + 2 * QA)};
+                butterfly<4, false>(y, wa, &wi, F);
+                v[t2] = y[0]; v[4 + t2] = y[1]; v[8 + t2] = y[2]; v[12 + t2] = y[3];
+            }
+        }
+#pragma unroll
+        for (int t1 = 0; t1 < 4; t1++)
+#pragma unroll
+            for (int t2 = 0; t2 < 4; t2++) s[sp(((row0 + t1 * 4 * q16 + t2 * q16) << T.lc) + c)] = v[t1 * 4 + t2];
+    }
+}
+
+// Radix-8 round: the span-8 radix-4 stage A (Q = 2) and the radix-2 stage, on
+// 8 consecutive points (contiguous passes only: C = 1, Qb = 1, j0 = 0).
+template <bool FWD>
+__device__ void round_r8(const Tiles& T, const DStage& A) {
+    const int per = T.G >> 3;
+    const int total = per * T.ntiles;
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        int tau;
+        const int b = split_unit(u, per, tau);
+        const int f = tau >> T.pshift;
+        const Fp F = fpctx(f);
+        const double wi = A.rot[f][0];
+        double* s = T.s + tau * T.stride;
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = s[sp(8 * b + k)];
+        const double* tw = A.tw[f];
+        const double w0[4] = {0.0, __ldg(tw + 0), __ldg(tw + 2), __ldg(tw + 4)};
+        const double w1[4] = {0.0, __ldg(tw + 1), __ldg(tw + 3), __ldg(tw + 5)};
+        if (!FWD) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) butterfly2(v[2 * i], v[2 * i + 1], F);
+        }
+        {
+            double y[4] = {v[0], v[2], v[4], v[6]};
+            butterfly<4, FWD>(y, w0, &wi, F);
+            v[0] = y[0]; v[2] = y[1]; v[4] = y[2]; v[6] = y[3];
+            double z[4] = {v[1], v[3], v[5], v[7]};
+            butterfly<4, FWD>(z, w1, &wi, F);
+            v[1] = z[0]; v[3] = z[1]; v[5] = z[2]; v[7] = z[3];
+        }
+        if (FWD) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) butterfly2(v[2 * i], v[2 * i + 1], F);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) s[sp(8 * b + k)] = v[k];
     }
 }
 
 template <bool FWD>
-__device__ void run_stage(double* s, const DStage& st, int f, int G, int lc, int64_t Qb, int64_t j0) {
-    const Fp F = fpctx(f);
-    const int Lloc = (int)(st.L / Qb);
-    const int Qloc = (int)(st.Q / Qb);
-    switch (st.m) {
-        case 2: stage_tile<2, FWD>(s, G, lc, Lloc, Qloc, nullptr, st.Q, Qb, j0, st.rot[f], F); break;
-        case 3: stage_tile<3, FWD>(s, G, lc, Lloc, Qloc, st.tw[f], st.Q, Qb, j0, st.rot[f], F); break;
-        case 4: stage_tile<4, FWD>(s, G, lc, Lloc, Qloc, st.tw[f], st.Q, Qb, j0, st.rot[f], F); break;
-        case 5: stage_tile<5, FWD>(s, G, lc, Lloc, Qloc, st.tw[f], st.Q, Qb, j0, st.rot[f], F); break;
-        default: stage_tile<7, FWD>(s, G, lc, Lloc, Qloc, st.tw[f], st.Q, Qb, j0, st.rot[f], F); break;
+__device__ void run_round(const Tiles& T, const DPlan& pl, int kind, int s0) {
+    __syncthreads();
+    const DStage& st = pl.st[s0];
+    switch (kind) {
+        case RK_R16: round_r16<FWD>(T, st, pl.st[s0 + 1]); break;
+        case RK_R8: round_r8<FWD>(T, st); break;
+        case RK_R4: round_gen<4, FWD>(T, st); break;
+        case RK_R2: round_gen<2, FWD>(T, st); break;
+        default:
+            if (st.m == 3) round_gen<3, FWD>(T, st);
+            else if (st.m == 5) round_gen<5, FWD>(T, st);
+            else round_gen<7, FWD>(T, st);
+            break;
     }
 }
 
 template <bool FWD>
-__device__ void run_pass(double* s, const DPlan& pl, const DPass& ps, int f, int64_t j0) {
-    const int lc = __ffs(ps.C) - 1;
+__device__ void run_pass(const Tiles& T, const DPlan& pl, const DPass& ps) {
     if (FWD) {
-        for (int i = ps.sa; i <= ps.sb; i++) {
-            __syncthreads();
-            run_stage<true>(s, pl.st[i], f, ps.G, lc, ps.Qb, j0);
-        }
+        for (int r = 0; r < ps.nrounds; r++) run_round<true>(T, pl, ps.rkind[r], ps.rstage[r]);
     } else {
-        for (int i = ps.sb; i >= ps.sa; i--) {
-            __syncthreads();
-            run_stage<false>(s, pl.st[i], f, ps.G, lc, ps.Qb, j0);
-        }
+        for (int r = ps.nrounds - 1; r >= 0; r--) run_round<false>(T, pl, ps.rkind[r], ps.rstage[r]);
     }
     __syncthreads();
 }
 
-// Tile geometry: tile t -> block offset o_a (multiple of L_sa) and first column j0.
-struct TileGeo {
-    int64_t base;  // o_a + j0
-    int64_t j0;
-};
-__device__ __forceinline__ TileGeo tile_geo(const DPlan& pl, const DPass& ps, int64_t t) {
-    int64_t per = ps.Qb / ps.C;
-    int64_t blk = t / per;
-    int64_t jc = t - blk * per;
-    TileGeo g;
-    g.j0 = jc * ps.C;
-    g.base = blk * pl.st[ps.sa].L + g.j0;
-    return g;
+// Tile geometry: tile t of pass ps -> global index of its (row 0, column 0) and its first column.
+__device__ __forceinline__ void tile_geo(const DPlan& pl, const DPass& ps, int64_t t, int& base, int& j0) {
+    const int per = (int)(ps.Qb / ps.C);
+    const int tt = (int)t;
+    const int blk = tt / per;
+    const int jc = tt - blk * per;
+    j0 = jc * ps.C;
+    base = blk * (int)pl.st[ps.sa].L + j0;
 }
 
-__device__ __forceinline__ void load_tile(double* s, const double* __restrict__ x, const DPass& ps, int64_t base) {
+// x[base + c + k*Qb] -> tile row k, column c (padded), for every tile t of the set reading x_t
+__device__ __forceinline__ void load_tile(double* s, const double* __restrict__ x, const DPass& ps, int base) {
     const int lc = __ffs(ps.C) - 1;
     const int n = ps.G << lc;
+    const int Qb = (int)ps.Qb;
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
-        int k = e >> lc, c = e & (ps.C - 1);
-        s[e] = x[base + c + (int64_t)k * ps.Qb];
+        const int k = e >> lc, c = e & (ps.C - 1);
+        s[sp(e)] = x[base + c + k * Qb];
     }
 }
-__device__ __forceinline__ void store_tile(const double* s, double* __restrict__ x, const DPass& ps, int64_t base) {
+__device__ __forceinline__ void store_tile(const double* s, double* __restrict__ x, const DPass& ps, int base) {
     const int lc = __ffs(ps.C) - 1;
     const int n = ps.G << lc;
+    const int Qb = (int)ps.Qb;
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
-        int k = e >> lc, c = e & (ps.C - 1);
-        x[base + c + (int64_t)k * ps.Qb] = s[e];
+        const int k = e >> lc, c = e & (ps.C - 1);
+        x[base + c + k * Qb] = s[sp(e)];
     }
 }
-__device__ __forceinline__ void pack_tile(double* s, const uint64_t* limbs, int64_t n, int b, int64_t nch,
-                                          const DPass& ps, int64_t base) {
+// one packed chunk written to both primes' tiles s0 and s1
+__device__ __forceinline__ void pack_tile2(double* s0, double* s1, const uint64_t* limbs, int64_t n, int b,
+                                           int64_t nch, const DPass& ps, int base) {
     const int lc = __ffs(ps.C) - 1;
     const int cnt = ps.G << lc;
+    const int Qb = (int)ps.Qb;
     for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
-        int k = e >> lc, c = e & (ps.C - 1);
-        s[e] = pack_chunk(limbs, n, b, nch, base + c + (int64_t)k * ps.Qb);
+        const int k = e >> lc, c = e & (ps.C - 1);
+        const double v = pack_chunk(limbs, n, b, nch, base + c + k * Qb);
+        s0[sp(e)] = v;
+        s1[sp(e)] = v;
     }
+}
+
+__device__ __forceinline__ Tiles make_tiles(double* s, int stride, int ntiles, int pshift, const DPass& ps, int j0) {
+    Tiles T;
+    T.s = s;
+    T.stride = stride;
+    T.ntiles = ntiles;
+    T.pshift = pshift;
+    T.G = ps.G;
+    T.lc = __ffs(ps.C) - 1;
+    T.Qb = (int)ps.Qb;
+    T.j0 = j0;
+    return T;
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_fwd(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
-                                             const Job* __restrict__ jobs, int64_t njobs) {
+// Forward pass of one tile of one operand, both primes (tiles X0, X1).
+__global__ void __launch_bounds__(PASS_THREADS, 2) k_fwd(const DProd* __restrict__ prods,
+                                                         const DPlan* __restrict__ plans,
+                                                         const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
         const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
-        const int f = jb.sub & 1, opb = (jb.sub >> 1) & 1, pass = (jb.sub >> 8) & 0xff;
+        const int opb = (jb.sub >> 1) & 1, pass = (jb.sub >> 8) & 0xff;
         const DPass& ps = pl.pass[pass];
-        const TileGeo g = tile_geo(pl, ps, jb.tile);
-        double* x = opb ? P.xb[f] : P.xa[f];
+        int base, j0;
+        tile_geo(pl, ps, jb.tile, base, j0);
+        const int stride = tile_stride_doubles(ps.G * ps.C);
+        double* s0 = smem;
+        double* s1 = smem + stride;
+        double* x0 = opb ? P.xb[0] : P.xa[0];
+        double* x1 = opb ? P.xb[1] : P.xa[1];
         __syncthreads();
         if (pass == 0 && !(P.flags & PF_PRELOADED)) {
-            if (opb) pack_tile(smem, P.b, P.n, P.bch, P.ncb, ps, g.base);
-            else pack_tile(smem, P.a, P.m, P.bch, P.nca, ps, g.base);
+            if (opb) pack_tile2(s0, s1, P.b, P.n, P.bch, P.ncb, ps, base);
+            else pack_tile2(s0, s1, P.a, P.m, P.bch, P.nca, ps, base);
         } else {
-            load_tile(smem, x, ps, g.base);
+            load_tile(s0, x0, ps, base);
+            load_tile(s1, x1, ps, base);
         }
-        run_pass<true>(smem, pl, ps, f, g.j0);
-        store_tile(smem, x, ps, g.base);
+        run_pass<true>(make_tiles(smem, stride, 2, 0, ps, j0), pl, ps);
+        store_tile(s0, x0, ps, base);
+        store_tile(s1, x1, ps, base);
     }
 }
 
-__global__ void __launch_bounds__(256) k_pwr(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
-                                             const Job* __restrict__ jobs, int64_t njobs) {
+// Last pass, both primes: forward on a (and b), pointwise, reverse on a.
+// Tiles: products [a0, b0, a1, b1], squares [a0, a1].
+__global__ void __launch_bounds__(PASS_THREADS, 2) k_pwr(const DProd* __restrict__ prods,
+                                                         const DPlan* __restrict__ plans,
+                                                         const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
         const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
-        const int f = jb.sub & 1;
         const int pass = P.npass - 1;
         const DPass& ps = pl.pass[pass];
-        const TileGeo g = tile_geo(pl, ps, jb.tile);
+        int base, j0;
+        tile_geo(pl, ps, jb.tile, base, j0);
+        const int stride = tile_stride_doubles(ps.G * ps.C);
+        const int sq = P.sqr;
+        double* a0 = smem;
+        double* a1 = smem + (sq ? 1 : 2) * stride;
+        double* b0 = sq ? a0 : smem + stride;
+        double* b1 = sq ? a1 : smem + 3 * stride;
         const int cnt = ps.G * ps.C;
-        double* sa = smem;
-        double* sb = smem + cnt;
         __syncthreads();
         if (pass == 0 && !(P.flags & PF_PRELOADED)) {
-            pack_tile(sa, P.a, P.m, P.bch, P.nca, ps, g.base);
-            if (!P.sqr) pack_tile(sb, P.b, P.n, P.bch, P.ncb, ps, g.base);
+            pack_tile2(a0, a1, P.a, P.m, P.bch, P.nca, ps, base);
+            if (!sq) pack_tile2(b0, b1, P.b, P.n, P.bch, P.ncb, ps, base);
         } else {
-            load_tile(sa, P.xa[f], ps, g.base);
-            if (!P.sqr) load_tile(sb, P.xb[f], ps, g.base);
+            load_tile(a0, P.xa[0], ps, base);
+            load_tile(a1, P.xa[1], ps, base);
+            if (!sq) {
+                load_tile(b0, P.xb[0], ps, base);
+                load_tile(b1, P.xb[1], ps, base);
+            }
         }
-        run_pass<true>(sa, pl, ps, f, g.j0);
-        if (!P.sqr) run_pass<true>(sb, pl, ps, f, g.j0);
-        const Fp F = fpctx(f);
-        if (P.sqr) {
-            for (int e = threadIdx.x; e < cnt; e += blockDim.x) sa[e] = fp_mulmod(sa[e], sa[e], F);
-        } else {
-            for (int e = threadIdx.x; e < cnt; e += blockDim.x) sa[e] = fp_mulmod(sa[e], sb[e], F);
+        run_pass<true>(make_tiles(smem, stride, sq ? 2 : 4, sq ? 0 : 1, ps, j0), pl, ps);
+        {
+            const Fp F0 = fpctx(0), F1 = fpctx(1);
+            for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+                const int i = sp(e);
+                a0[i] = fp_mulmod(a0[i], b0[i], F0);
+                a1[i] = fp_mulmod(a1[i], b1[i], F1);
+            }
         }
-        run_pass<false>(sa, pl, ps, f, g.j0);
-        store_tile(sa, P.xa[f], ps, g.base);
+        run_pass<false>(make_tiles(a0, (int)(a1 - a0), 2, 0, ps, j0), pl, ps);
+        store_tile(a0, P.xa[0], ps, base);
+        store_tile(a1, P.xa[1], ps, base);
     }
 }
 
-__global__ void __launch_bounds__(256) k_rev(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
-                                             const Job* __restrict__ jobs, int64_t njobs) {
+// Reverse pass of one tile, both primes.
+__global__ void __launch_bounds__(PASS_THREADS, 2) k_rev(const DProd* __restrict__ prods,
+                                                         const DPlan* __restrict__ plans,
+                                                         const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
         const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
-        const int f = jb.sub & 1, pass = (jb.sub >> 8) & 0xff;
+        const int pass = (jb.sub >> 8) & 0xff;
         const DPass& ps = pl.pass[pass];
-        const TileGeo g = tile_geo(pl, ps, jb.tile);
+        int base, j0;
+        tile_geo(pl, ps, jb.tile, base, j0);
+        const int stride = tile_stride_doubles(ps.G * ps.C);
         __syncthreads();
-        load_tile(smem, P.xa[f], ps, g.base);
-        run_pass<false>(smem, pl, ps, f, g.j0);
-        store_tile(smem, P.xa[f], ps, g.base);
+        load_tile(smem, P.xa[0], ps, base);
+        load_tile(smem + stride, P.xa[1], ps, base);
+        run_pass<false>(make_tiles(smem, stride, 2, 0, ps, j0), pl, ps);
+        store_tile(smem, P.xa[0], ps, base);
+        store_tile(smem + stride, P.xa[1], ps, base);
     }
 }
 

@@ -59,8 +59,8 @@ static std::mutex g_na_mu;
 // host-side power tables for one twiddle build (nhi <= 4096 entries at the largest admitted length)
 static double g_na_hilo[4096 + 4096];
 
-// jobs[i] for one launch over all primes and operands of a single product:
-// i = ((f * nops) + op) * ntiles + t
+// jobs[i] for one launch over the operands of a single product (pass jobs
+// cover both primes; nprimes is 1 for them): i = ((f * nops) + op) * ntiles + t
 __global__ void k_noalloc_jobs(Job* __restrict__ jobs, int64_t ntiles, int nprimes, int nops, int pass) {
     const int64_t n = ntiles * nprimes * nops;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -153,8 +153,9 @@ extern "C" int nbg_mul_dev_noalloc(uint64_t* r, const uint64_t* a, int64_t m, co
     const int64_t nhi = (N + 4095) / 4096;
     const int nops = sqr ? 1 : 2;
     int64_t njobs = 0;
-    for (int p = 0; p < P - 1; p++) njobs += 2 * nops * d.pass[p].ntiles + 2 * d.pass[p].ntiles;
-    njobs += 2 * d.pass[P - 1].ntiles;
+    // pass jobs cover one tile of both primes
+    for (int p = 0; p < P - 1; p++) njobs += nops * d.pass[p].ntiles + d.pass[p].ntiles;
+    njobs += d.pass[P - 1].ntiles;
     const int64_t rn = m + n;
     const int64_t ntl = (rn + UNPACK_TL - 1) / UNPACK_TL;
     njobs += ntl + 1;
@@ -288,18 +289,21 @@ extern "C" int nbg_mul_dev_noalloc(uint64_t* r, const uint64_t* a, int64_t m, co
     };
     for (int p = 0; p < P - 1; p++) {
         const DPass& ps = d.pass[p];
-        NA_TRY(fill(ps.ntiles, 2, nops, p));
-        NA_TRY(run(JK_FWD, 2 * nops * ps.ntiles, sizeof(double) * (size_t)ps.G * ps.C));
+        const size_t tile = sizeof(double) * (size_t)tile_stride_doubles(ps.G * ps.C);
+        NA_TRY(fill(ps.ntiles, 1, nops, p));
+        NA_TRY(run(JK_FWD, nops * ps.ntiles, 2 * tile));
     }
     {
         const DPass& ps = d.pass[P - 1];
-        NA_TRY(fill(ps.ntiles, 2, 1, P - 1));
-        NA_TRY(run(JK_PWR, 2 * ps.ntiles, sizeof(double) * (size_t)ps.G * ps.C * nops));
+        const size_t tile = sizeof(double) * (size_t)tile_stride_doubles(ps.G * ps.C);
+        NA_TRY(fill(ps.ntiles, 1, 1, P - 1));
+        NA_TRY(run(JK_PWR, ps.ntiles, 2 * nops * tile));
     }
     for (int p = P - 2; p >= 0; p--) {
         const DPass& ps = d.pass[p];
-        NA_TRY(fill(ps.ntiles, 2, 1, p));
-        NA_TRY(run(JK_REV, 2 * ps.ntiles, sizeof(double) * (size_t)ps.G * ps.C));
+        const size_t tile = sizeof(double) * (size_t)tile_stride_doubles(ps.G * ps.C);
+        NA_TRY(fill(ps.ntiles, 1, 1, p));
+        NA_TRY(run(JK_REV, ps.ntiles, 2 * tile));
     }
     const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / bch + 4;
     NA_TRY(fill(ntl, 1, 1, 0));

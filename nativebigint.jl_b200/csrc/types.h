@@ -15,6 +15,12 @@
 #pragma once
 #include <cstdint>
 
+#ifdef __CUDACC__
+#define NBG_HD __host__ __device__
+#else
+#define NBG_HD
+#endif
+
 namespace nbg {
 
 constexpr int MAXST = 24;    // 4 odd + 17 radix-4 + radix-2 at N = 315*2^34
@@ -29,12 +35,24 @@ struct DStage {
     double rot[2][8];    // per prime combine constants (radix-4: rot[0] = wi)
 };
 
+// Round kinds: how a pass's stages are executed in shared memory.
+enum RoundKind : int8_t {
+    RK_ODD = 0,  // one radix-3/5/7 stage, one butterfly per work unit
+    RK_R4 = 1,   // one radix-4 stage
+    RK_R16 = 2,  // radix-4 stages s (span L) and s+1 (span L/4) on 16 registers per unit
+    RK_R8 = 3,   // radix-4 stage s (span 8) and the radix-2 stage s+1 on 8 registers per unit
+    RK_R2 = 4,   // a lone radix-2 stage
+};
+
 struct DPass {
     int32_t sa, sb;      // stage range, inclusive
     int32_t G;           // rows per tile = L_sa / Q_sb
     int32_t C;           // columns per tile (power of two dividing Qb)
     int64_t Qb;          // column stride = Q_sb
     int64_t ntiles;      // (N / L_sa) * (Qb / C)
+    int32_t nrounds;
+    int8_t rkind[MAXST]; // forward order; the reverse runs them backwards
+    int8_t rstage[MAXST];// first stage of each round
 };
 
 struct DPlan {
@@ -65,7 +83,9 @@ struct DProd {
 };
 
 // Work item of one launch.  kind-specific meaning of `sub`:
-//   bit 0 prime, bit 1 operand (0 = a, 1 = b); pass index in bits 8..15.
+//   k_fwd: bit 1 operand (0 = a, 1 = b), pass index in bits 8..15
+//   k_rev: pass index in bits 8..15
+//   (pass kernels process both primes of a tile; unpack/carry ignore `sub`).
 struct Job {
     int32_t prod;
     int32_t sub;
@@ -81,6 +101,12 @@ enum JobKind : int32_t {
 };
 
 constexpr int UNPACK_TL = 1024;  // output limbs per unpack tile
+constexpr int PASS_THREADS = 256;
+
+// Shared-memory tiles are padded by one double every 16 so that strided
+// accesses of the radix-16/8 rounds fall in distinct banks.
+NBG_HD inline int tile_pad_index(int i) { return i + (i >> 4); }
+NBG_HD inline int tile_stride_doubles(int n) { return ((n + (n >> 4) + 1) + 1) & ~1; }
 
 // DProd.flags
 constexpr int32_t PF_PRELOADED = 1;  // pass 0 loads xa/xb as-is instead of packing limbs

@@ -88,7 +88,8 @@ def lib() -> ctypes.CDLL:
             "nbg_pointwise_dev": [vp, vp, i64, i32, vp],
             "nbg_unpack_dev": [vp, i64, vp, vp, i64, i64, i32, vp],
             "nbg_plan_info": [i64, c.POINTER(i32), c.POINTER(i32), c.POINTER(i32), c.POINTER(i32), i32],
-            "nbg_plan_layout": [i64, i32, c.POINTER(i64), c.POINTER(i32), c.POINTER(i64), c.POINTER(i32), i32],
+            "nbg_plan_layout": [i64, i32, c.POINTER(i64), c.POINTER(i32), c.POINTER(i64), c.POINTER(i32),
+                                c.POINTER(i32), i32],
             "nbg_set_tuning": [c.c_char_p],
             "nbg_get_tuning": [c.c_char_p, i64],
             "nbg_init": [i32],
@@ -324,16 +325,23 @@ def plan_info(N: int) -> dict:
     return {"stages": list(sm[: nst.value]), "pass_end": list(pe[: npass.value])}
 
 
+ROUND_KINDS = {0: "odd", 1: "r4", 2: "r16", 3: "r8", 4: "r2"}
+
+
 def plan_layout(N: int, sqr: bool = False) -> dict:
-    """Stages (m, L, Q) and passes (sa, sb, G, C, Qb, ntiles) for length N; host only."""
+    """Stages (m, L, Q), passes (sa, sb, G, C, Qb, ntiles) and each pass's
+    rounds [(kind, first stage)] for length N; host only."""
     cap = 32
     st = (ctypes.c_int64 * (3 * cap))()
-    ps = (ctypes.c_int64 * (6 * cap))()
+    ps = (ctypes.c_int64 * (7 * cap))()
+    rd = (ctypes.c_int32 * (cap * cap))()
     nst, npass = ctypes.c_int32(), ctypes.c_int32()
-    _check(lib().nbg_plan_layout(N, 1 if sqr else 0, st, ctypes.byref(nst), ps, ctypes.byref(npass), cap))
+    _check(lib().nbg_plan_layout(N, 1 if sqr else 0, st, ctypes.byref(nst), ps, ctypes.byref(npass), rd, cap))
     stages = [tuple(st[3 * i: 3 * i + 3]) for i in range(nst.value)]
-    passes = [tuple(ps[6 * j: 6 * j + 6]) for j in range(npass.value)]
-    return {"stages": stages, "passes": passes}
+    passes = [tuple(ps[7 * j: 7 * j + 6]) for j in range(npass.value)]
+    rounds = [[(ROUND_KINDS[rd[j * cap + r] >> 8], rd[j * cap + r] & 0xff) for r in range(ps[7 * j + 6])]
+              for j in range(npass.value)]
+    return {"stages": stages, "passes": passes, "rounds": rounds}
 
 
 def set_tuning(js: str) -> None:

@@ -100,10 +100,21 @@ def test_dispatch_thresholds():
 # butterfly a tile runs is the reference's butterfly (same global lanes, same
 # twiddle column) for its stage (fp_stage!, src/fpntt.jl:703-713).
 
+def _pad(i):
+    return i + (i >> 4)
+
+
+def _stride(n):
+    return ((n + (n >> 4) + 1) + 1) & ~1
+
+
 def _emulate_plan(N, layout):
-    stages, passes = layout["stages"], layout["passes"]
-    covered_stage = {s: 0 for s in range(len(stages))}
-    for (sa, sb, G, C, Qb, ntiles) in passes:
+    """Emulates the pass kernels' index arithmetic (round_gen, round_r16,
+    round_r8, tile loads/stores) with numpy and checks it against the
+    reference's enumeration of butterflies."""
+    stages, passes, rounds = layout["stages"], layout["passes"], layout["rounds"]
+    seen = {s: [] for s in range(len(stages))}
+    for (sa, sb, G, C, Qb, ntiles), rds in zip(passes, rounds):
         assert C & (C - 1) == 0 and Qb % C == 0 and G * C <= 8192
         La = stages[sa][1]
         assert La % Qb == 0 and La // Qb == G
@@ -111,49 +122,105 @@ def _emulate_plan(N, layout):
         t = np.arange(ntiles, dtype=np.int64)
         blk, jc = t // per, t % per
         j0 = jc * C
-        base = blk * La + j0
+        tbase = blk * La + j0
         k = np.arange(G, dtype=np.int64)[:, None]
         c = np.arange(C, dtype=np.int64)[None, :]
-        idx = base[:, None, None] + c[None] + k[None] * Qb  # (tile, k, c)
-        flat = idx.ravel()
-        assert flat.min() >= 0 and flat.max() < N
-        assert np.array_equal(np.sort(flat), np.arange(N))
+        idx = tbase[:, None, None] + c[None] + k[None] * Qb
+        assert idx.min() >= 0 and idx.max() < N
+        assert np.array_equal(np.sort(idx.ravel()), np.arange(N))
         lc = C.bit_length() - 1
-        for s in range(sa, sb + 1):
+        ntile_elems = G * C
+        assert _pad(ntile_elems - 1) < _stride(ntile_elems)
+
+        def glob(local):  # tile-local element index -> global index, per tile
+            assert local.min() >= 0 and local.max() < ntile_elems
+            assert _pad(local).max() < _stride(ntile_elems)
+            kk, c2 = local >> lc, local & (C - 1)
+            return tbase[:, None] + c2[None, :] + kk[None, :] * Qb
+
+        def check(s, lanes, jcol):
             m, Ls, Qs = stages[s]
-            Lloc, Qloc = Ls // Qb, Qs // Qb
-            nb = (G // m) * C
-            e = np.arange(nb, dtype=np.int64)
-            cc, row = e & (C - 1), e >> lc
-            blk_l, jl = row // Qloc, row % Qloc
-            lbase = ((blk_l * Lloc + jl) << lc) + cc
-            stride = Qloc << lc
-            jt = jl[None, :] * Qb + j0[:, None] + cc[None, :]  # twiddle column per tile
-            assert jt.min() >= 0 and jt.max() < Qs
-            lanes = []
-            for tl in range(m):
-                l = lbase + tl * stride
-                assert l.max() < G * C
-                kk, c2 = l >> lc, l & (C - 1)
-                lanes.append(base[:, None] + c2[None, :] + kk[None, :] * Qb)
             g0 = lanes[0]
-            # reference butterfly: lanes at o + j + t*Q_s with j = g0 mod L_s, j < Q_s
-            assert np.array_equal(g0 % Ls, jt)
+            assert np.array_equal(g0 % Ls, jcol) and jcol.max() < Qs
             for tl in range(1, m):
                 assert np.array_equal(lanes[tl], g0 + tl * Qs)
-            covered_stage[s] += g0.size
-        for s in range(sa, sb + 1):
-            assert covered_stage[s] == N // stages[s][0]
-    assert [st for st in covered_stage.values()] == [N // s[0] for s in stages]
+            seen[s].append(g0.ravel())
+
+        stage_set = set()
+        for kind, s in rds:
+            if kind in ("odd", "r4", "r2"):
+                m, Ls, Qs = stages[s]
+                Lloc, Qloc = Ls // Qb, Qs // Qb
+                e = np.arange((G // m) * C, dtype=np.int64)
+                cc, row = e & (C - 1), e >> lc
+                # multiply-high division of the kernel: (row >> e2) * mg >> 32
+                e2 = (Qloc & -Qloc).bit_length() - 1
+                odd = Qloc >> e2
+                rs = row >> e2
+                if odd == 1:
+                    bl = rs
+                else:
+                    mg = (0xFFFFFFFF // odd) + 1
+                    bl = (rs * mg) >> 32
+                assert np.array_equal(bl, row // Qloc)
+                jl = row - bl * Qloc
+                lb = ((bl * Lloc + jl) << lc) + cc
+                lanes = [glob(lb + tl * (Qloc << lc)) for tl in range(m)]
+                jcol = (jl * Qb)[None, :] + j0[:, None] + cc[None, :]
+                check(s, lanes, jcol)
+                stage_set.add(s)
+            elif kind == "r16":
+                mA, LA, QA = stages[s]
+                mB, LB, QB = stages[s + 1]
+                assert mA == 4 and mB == 4 and LB * 4 == LA
+                Lloc = LA // Qb
+                q16 = Lloc >> 4
+                assert q16 >= 1 and q16 & (q16 - 1) == 0
+                lq = q16.bit_length() - 1
+                e = np.arange((G >> 4) * C, dtype=np.int64)
+                cc, r = e & (C - 1), e >> lc
+                b, j2 = r >> lq, r & (q16 - 1)
+                row0 = b * Lloc + j2
+                loc = lambda t1, t2: ((row0 + t1 * 4 * q16 + t2 * q16) << lc) + cc
+                for t2 in range(4):
+                    lanes = [glob(loc(t1, t2)) for t1 in range(4)]
+                    jA = ((j2 + t2 * q16) * Qb)[None, :] + j0[:, None] + cc[None, :]
+                    check(s, lanes, jA)
+                for t1 in range(4):
+                    lanes = [glob(loc(t1, t2)) for t2 in range(4)]
+                    jB = (j2 * Qb)[None, :] + j0[:, None] + cc[None, :]
+                    check(s + 1, lanes, jB)
+                stage_set |= {s, s + 1}
+            elif kind == "r8":
+                assert C == 1 and Qb == 1
+                mA, LA, QA = stages[s]
+                assert (mA, LA, QA) == (4, 8, 2) and stages[s + 1][0] == 2
+                b = np.arange(G >> 3, dtype=np.int64)
+                for j in range(2):
+                    lanes = [glob(8 * b + j + 2 * tl) for tl in range(4)]
+                    check(s, lanes, np.full((ntiles, b.size), j))
+                for i in range(4):
+                    lanes = [glob(8 * b + 2 * i + tl) for tl in range(2)]
+                    check(s + 1, lanes, np.zeros((ntiles, b.size), dtype=np.int64))
+                stage_set |= {s, s + 1}
+            else:
+                raise AssertionError(kind)
+        assert stage_set == set(range(sa, sb + 1))
+    for s, (m, Ls, Qs) in enumerate(stages):
+        g0 = np.sort(np.concatenate(seen[s]))
+        # every butterfly of the stage exactly once: lane-0 indices o + j, o = k*L, j < Q
+        want = (np.arange(N // Ls)[:, None] * Ls + np.arange(Qs)[None, :]).ravel()
+        assert np.array_equal(g0, np.sort(want)), s
     assert passes[-1][4] == 1 and passes[-1][1] == len(stages) - 1
 
 
 EMU_N = (4, 8, 12, 48, 240, 420, 1260, 4032, 960, 1680, 12288, 20480, 7 * 2**15, 9 * 2**11, 105 * 2**11,
          2**16, 315 * 2**10, 63 * 2**12, 45 * 2**11, 2**17 * 3)
 EMU_TUNINGS = (None,
-               '{"full_max_mul": 4, "full_max_sqr": 4, "last_max": 4, "early_gmax": 2, "tile_target": 8, "cmax": 2}',
-               '{"full_max_mul": 16, "full_max_sqr": 16, "last_max": 64, "early_gmax": 16, "tile_target": 64, "cmax": 8}',
-               '{"full_max_mul": 256, "full_max_sqr": 256, "last_max": 256, "early_gmax": 64, "tile_target": 512, "cmax": 32}')
+               '{"full_max_mul": 4, "full_max_sqr": 4, "last_max": 4, "last_max_sqr": 4, "early_gmax": 2, "tile_target": 8, "cmax": 2}',
+               '{"full_max_mul": 16, "full_max_sqr": 16, "last_max": 64, "last_max_sqr": 32, "early_gmax": 16, "tile_target": 64, "cmax": 8}',
+               '{"full_max_mul": 256, "full_max_sqr": 256, "last_max": 256, "last_max_sqr": 512, "early_gmax": 64, "tile_target": 512, "cmax": 32}',
+               '{"full_max_mul": 4096, "full_max_sqr": 8192, "last_max": 4096, "last_max_sqr": 8192, "early_gmax": 1024, "tile_target": 4096, "cmax": 128}')
 
 
 @pytest.mark.parametrize("tun", EMU_TUNINGS)
@@ -174,7 +241,7 @@ def test_large_plan_layouts():
         lay = nbgpu.plan_layout(N)
         assert 2 <= len(lay["passes"]) <= 6
         for (sa, sb, G, C, Qb, nt) in lay["passes"]:
-            assert G * C * 8 * 2 <= 227 * 1024
+            assert 4 * _stride(G * C) * 8 <= 227 * 1024
     _emulate_plan(315 * 2**14, nbgpu.plan_layout(315 * 2**14))
 
 

@@ -679,12 +679,25 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         for (int64_t t = 0; t < P.ntl; t++) unp.push_back(Job{(int32_t)k, 0, t});
         if (P.ntl > 1) car.push_back(Job{(int32_t)k, 0, 0});
     }
-    // biggest pointwise tiles first so the tail of the launch is short
-    std::stable_sort(pwr.begin(), pwr.end(), [&](const Job& x, const Job& y) {
-        const DPlan& px = bb.plan_of[(size_t)x.prod]->d;
-        const DPlan& py = bb.plan_of[(size_t)y.prod]->d;
-        return px.pass[bb.prods[(size_t)x.prod].npass - 1].G > py.pass[bb.prods[(size_t)y.prod].npass - 1].G;
-    });
+    // Order jobs so CTAs that run together share twiddle columns: by plan
+    // (transform length), then tile, then product.  Every product of one
+    // length reads the same twiddle slice for the same tile, so the slice is
+    // fetched from DRAM once and served from L2 to the rest.  Biggest plans
+    // first so the tail of each launch is short.
+    auto by_plan_tile = [&](std::vector<Job>& v) {
+        std::stable_sort(v.begin(), v.end(), [&](const Job& x, const Job& y) {
+            const DPlan& px = bb.plan_of[(size_t)x.prod]->d;
+            const DPlan& py = bb.plan_of[(size_t)y.prod]->d;
+            if (px.N != py.N) return px.N > py.N;
+            const int sx = bb.prods[(size_t)x.prod].plan, sy = bb.prods[(size_t)y.prod].plan;
+            if (sx != sy) return sx < sy;
+            if (x.tile != y.tile) return x.tile < y.tile;
+            return x.sub < y.sub;
+        });
+    };
+    for (auto& v : fwd) by_plan_tile(v);
+    for (auto& v : rev) by_plan_tile(v);
+    by_plan_tile(pwr);
     auto add = [&](int kind, std::vector<Job>& v, size_t smem, double ops, double bytes) {
         if (v.empty()) return;
         Launch L{kind, (int64_t)bb.jobs.size(), (int64_t)v.size(), smem};

@@ -93,11 +93,15 @@ __device__ void round_gen(const Tiles& T, const DStage& st) {
     const unsigned odd = (unsigned)(Qloc >> e);
     const unsigned mg = odd == 1 ? 0u : 0xFFFFFFFFu / odd + 1u;
     const int stride = Qloc << T.lc;
+    // per-prime constants, loaded once per round
+    const Fp F0 = fpctx(0), F1 = fpctx(1);
+    const double* tw0 = st.tw[0];
+    const double* tw1 = st.tw[1];
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
         int tau;
         const int uu = split_unit(u, per, tau);
-        const int f = tau >> T.pshift;
-        const Fp F = fpctx(f);
+        const bool p1 = (tau >> T.pshift) != 0;
+        const Fp F = p1 ? F1 : F0;
         double* s = T.s + tau * T.stride;
         const int c = uu & (C - 1);
         const int row = uu >> T.lc;
@@ -112,14 +116,16 @@ __device__ void round_gen(const Tiles& T, const DStage& st) {
             butterfly2(y[0], y[1], F);
         } else {
             const int j = jl * T.Qb + T.j0 + c;
-            const double* tw = st.tw[f] + j;
+            const double* tw = (p1 ? tw1 : tw0) + j;
             double w[M];
             w[0] = 0.0;
 #pragma unroll
             for (int t = 1; t < M; t++) w[t] = __ldg(tw + (t - 1) * Q);
+            constexpr int NR = M == 3 ? 1 : (M == 5 ? 4 : (M == 4 ? 1 : 8));
             double rot[8];
+            const double* rp = st.rot[p1 ? 1 : 0];
 #pragma unroll
-            for (int t = 0; t < 8; t++) rot[t] = st.rot[f][t];
+            for (int t = 0; t < NR; t++) rot[t] = rp[t];
             butterfly<M, FWD>(y, w, rot, F);
         }
 #pragma unroll
@@ -139,12 +145,14 @@ __device__ void round_r16(const Tiles& T, const DStage& A, const DStage& B) {
     const int QA = (int)A.Q, QB = (int)B.Q;
     const int per = (T.G >> 4) << T.lc;
     const int total = per * T.ntiles;
+    const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];  // the same 4th root for every radix-4 stage
+    const double *twA0 = A.tw[0], *twA1 = A.tw[1], *twB0 = B.tw[0], *twB1 = B.tw[1];
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
         int tau;
         const int uu = split_unit(u, per, tau);
-        const int f = tau >> T.pshift;
-        const Fp F = fpctx(f);
-        const double wi = A.rot[f][0];  // the same 4th root for every radix-4 stage
+        const bool p1 = (tau >> T.pshift) != 0;
+        const Fp F = fpctx(p1 ? 1 : 0);
+        const double wi = p1 ? wi1 : wi0;
         double* s = T.s + tau * T.stride;
         const int c = uu & (C - 1);
         const int r = uu >> T.lc;
@@ -156,8 +164,8 @@ __device__ void round_r16(const Tiles& T, const DStage& A, const DStage& B) {
 #pragma unroll
             for (int t2 = 0; t2 < 4; t2++) v[t1 * 4 + t2] = s[sp(((row0 + t1 * 4 * q16 + t2 * q16) << T.lc) + c)];
         const int jB = j2 * T.Qb + T.j0 + c;
-        const double* twB = B.tw[f] + jB;
-        const double* twA = A.tw[f] + jB;  // A's column for t2 is jB + t2*q16*Qb
+        const double* twB = (p1 ? twB1 : twB0) + jB;
+        const double* twA = (p1 ? twA1 : twA0) + jB;  // A's column for t2 is jB + t2*q16*Qb
         const int stepA = q16 * T.Qb;
         if (FWD) {
 #pragma unroll
@@ -197,17 +205,20 @@ template <bool FWD>
 __device__ void round_r8(const Tiles& T, const DStage& A) {
     const int per = T.G >> 3;
     const int total = per * T.ntiles;
+    const Fp F0 = fpctx(0), F1 = fpctx(1);
+    const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
+    const double *tw0 = A.tw[0], *tw1 = A.tw[1];
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
         int tau;
         const int b = split_unit(u, per, tau);
-        const int f = tau >> T.pshift;
-        const Fp F = fpctx(f);
-        const double wi = A.rot[f][0];
+        const bool p1 = (tau >> T.pshift) != 0;
+        const Fp F = p1 ? F1 : F0;
+        const double wi = p1 ? wi1 : wi0;
         double* s = T.s + tau * T.stride;
         double v[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) v[k] = s[sp(8 * b + k)];
-        const double* tw = A.tw[f];
+        const double* tw = p1 ? tw1 : tw0;
         const double w0[4] = {0.0, __ldg(tw + 0), __ldg(tw + 2), __ldg(tw + 4)};
         const double w1[4] = {0.0, __ldg(tw + 1), __ldg(tw + 3), __ldg(tw + 5)};
         if (!FWD) {
@@ -268,36 +279,79 @@ __device__ __forceinline__ void tile_geo(const DPlan& pl, const DPass& ps, int64
     base = blk * (int)pl.st[ps.sa].L + j0;
 }
 
-// x[base + c + k*Qb] -> tile row k, column c (padded), for every tile t of the set reading x_t
-__device__ __forceinline__ void load_tile(double* s, const double* __restrict__ x, const DPass& ps, int base) {
+// Asynchronous global -> shared copies (cp.async, 8 bytes each): a thread
+// issues every copy of its share of the tile set before waiting once, so the
+// loads of a whole tile are in flight together instead of one per thread.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// x[base + c + k*Qb] -> tile row k, column c (padded).  Issues only; the
+// caller waits with cp_async_wait_all() and a barrier.
+__device__ __forceinline__ void load_tile_async(double* s, const double* __restrict__ x, const DPass& ps, int base) {
     const int lc = __ffs(ps.C) - 1;
     const int n = ps.G << lc;
     const int Qb = (int)ps.Qb;
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
         const int k = e >> lc, c = e & (ps.C - 1);
-        s[sp(e)] = x[base + c + k * Qb];
+        cp_async8(s + sp(e), x + base + c + k * Qb);
     }
 }
 __device__ __forceinline__ void store_tile(const double* s, double* __restrict__ x, const DPass& ps, int base) {
     const int lc = __ffs(ps.C) - 1;
     const int n = ps.G << lc;
     const int Qb = (int)ps.Qb;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-        const int k = e >> lc, c = e & (ps.C - 1);
-        x[base + c + k * Qb] = s[sp(e)];
+    const int nt = blockDim.x;
+    int e = threadIdx.x;
+    // batches of 4 shared loads ahead of their global stores
+    for (; e + 3 * nt < n; e += 4 * nt) {
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) v[q] = s[sp(e + q * nt)];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int ee = e + q * nt;
+            x[base + (ee & (ps.C - 1)) + (ee >> lc) * Qb] = v[q];
+        }
     }
+    for (; e < n; e += nt) x[base + (e & (ps.C - 1)) + (e >> lc) * Qb] = s[sp(e)];
 }
-// one packed chunk written to both primes' tiles s0 and s1
-__device__ __forceinline__ void pack_tile2(double* s0, double* s1, const uint64_t* limbs, int64_t n, int b,
-                                           int64_t nch, const DPass& ps, int base) {
+// one packed chunk written to both primes' tiles s0 and s1; chunks are
+// processed 4 per thread at a time so their limb loads overlap
+__device__ __forceinline__ void pack_tile2(double* s0, double* s1, const uint64_t* __restrict__ limbs, int64_t n,
+                                           int b, int64_t nch, const DPass& ps, int base) {
     const int lc = __ffs(ps.C) - 1;
     const int cnt = ps.G << lc;
     const int Qb = (int)ps.Qb;
-    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
-        const int k = e >> lc, c = e & (ps.C - 1);
-        const double v = pack_chunk(limbs, n, b, nch, base + c + k * Qb);
-        s0[sp(e)] = v;
-        s1[sp(e)] = v;
+    const int nt = blockDim.x;
+    const uint64_t mask = (1ULL << b) - 1ULL;
+    for (int e0 = threadIdx.x; e0 < cnt; e0 += 4 * nt) {
+        uint64_t lo[4], hi[4];
+        int sh[4];
+        bool live[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int e = e0 + q * nt;
+            const int64_t i = e < cnt ? (int64_t)base + (e & (ps.C - 1)) + (int64_t)(e >> lc) * Qb : nch;
+            live[q] = i < nch;
+            const uint64_t bit = (uint64_t)(live[q] ? i : 0) * (uint32_t)b;
+            const int64_t w = (int64_t)(bit >> 6);
+            sh[q] = (int)(bit & 63);
+            lo[q] = live[q] ? __ldg(limbs + w) : 0;
+            hi[q] = (live[q] && sh[q] + b > 64 && w + 1 < n) ? __ldg(limbs + w + 1) : 0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int e = e0 + q * nt;
+            if (e >= cnt) break;
+            uint64_t c = lo[q] >> sh[q];
+            if (sh[q]) c |= hi[q] << (64 - sh[q]);
+            const double v = live[q] ? small_u64_to_double(c & mask) : 0.0;
+            s0[sp(e)] = v;
+            s1[sp(e)] = v;
+        }
     }
 }
 
@@ -338,8 +392,9 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) k_fwd(const DProd* __restrict
             if (opb) pack_tile2(s0, s1, P.b, P.n, P.bch, P.ncb, ps, base);
             else pack_tile2(s0, s1, P.a, P.m, P.bch, P.nca, ps, base);
         } else {
-            load_tile(s0, x0, ps, base);
-            load_tile(s1, x1, ps, base);
+            load_tile_async(s0, x0, ps, base);
+            load_tile_async(s1, x1, ps, base);
+            cp_async_wait_all();
         }
         run_pass<true>(make_tiles(smem, stride, 2, 0, ps, j0), pl, ps);
         store_tile(s0, x0, ps, base);
@@ -373,12 +428,13 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) k_pwr(const DProd* __restrict
             pack_tile2(a0, a1, P.a, P.m, P.bch, P.nca, ps, base);
             if (!sq) pack_tile2(b0, b1, P.b, P.n, P.bch, P.ncb, ps, base);
         } else {
-            load_tile(a0, P.xa[0], ps, base);
-            load_tile(a1, P.xa[1], ps, base);
+            load_tile_async(a0, P.xa[0], ps, base);
+            load_tile_async(a1, P.xa[1], ps, base);
             if (!sq) {
-                load_tile(b0, P.xb[0], ps, base);
-                load_tile(b1, P.xb[1], ps, base);
+                load_tile_async(b0, P.xb[0], ps, base);
+                load_tile_async(b1, P.xb[1], ps, base);
             }
+            cp_async_wait_all();
         }
         run_pass<true>(make_tiles(smem, stride, sq ? 2 : 4, sq ? 0 : 1, ps, j0), pl, ps);
         {
@@ -410,8 +466,9 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) k_rev(const DProd* __restrict
         tile_geo(pl, ps, jb.tile, base, j0);
         const int stride = tile_stride_doubles(ps.G * ps.C);
         __syncthreads();
-        load_tile(smem, P.xa[0], ps, base);
-        load_tile(smem + stride, P.xa[1], ps, base);
+        load_tile_async(smem, P.xa[0], ps, base);
+        load_tile_async(smem + stride, P.xa[1], ps, base);
+        cp_async_wait_all();
         run_pass<false>(make_tiles(smem, stride, 2, 0, ps, j0), pl, ps);
         store_tile(smem, P.xa[0], ps, base);
         store_tile(smem + stride, P.xa[1], ps, base);

@@ -47,12 +47,19 @@ WORKLOAD = "10,000 mixed products: larger operand log-uniform [152, 65536] limbs
 # ---------------------------------------------------------------------------
 # workload
 
-def gen_workload(seed: int, count: int):
+def gen_workload(seed: int, count: int, shape: tuple[int, int] | None = None, square: bool = False):
+    """The mixed 10,000-product batch; or, with `shape`, `count` copies of one
+    m x n shape (all squares with `square`), for per-class profiling."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    m = np.exp(rng.uniform(math.log(152), math.log(65536), count)).astype(np.int64)
-    ratio = rng.uniform(0.25, 1.0, count)
-    n = np.maximum(1, np.round(m * ratio).astype(np.int64))
-    sq = rng.random(count) < 0.2
+    if shape:
+        m = np.full(count, shape[0], dtype=np.int64)
+        n = np.full(count, shape[1], dtype=np.int64)
+        sq = np.full(count, bool(square))
+    else:
+        m = np.exp(rng.uniform(math.log(152), math.log(65536), count)).astype(np.int64)
+        ratio = rng.uniform(0.25, 1.0, count)
+        n = np.maximum(1, np.round(m * ratio).astype(np.int64))
+        sq = rng.random(count) < 0.2
     n = np.where(sq, m, n)
     # operand limbs, one flat array: a_k then (for products) b_k
     la = m.copy()
@@ -251,7 +258,8 @@ def run_ours(args, rank: int, world: int) -> None:
     torch.cuda.set_device(dev)
     nbgpu._check(nbgpu.lib().nbg_init(dev))
     stream = torch.cuda.Stream()
-    W = gen_workload(args.seed + rank, args.products)
+    shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else None
+    W = gen_workload(args.seed + rank, args.products, shape, args.square)
     count = args.products
     limbs = W["limbs"]
     d_in = torch.from_numpy(limbs).to(f"cuda:{dev}")
@@ -440,6 +448,8 @@ def main() -> None:
     ap.add_argument("--check", type=int, default=64, help="products verified against GMP after timing")
     ap.add_argument("--unbatched", type=int, default=10000, help="products issued one per call")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--shape", default="", help="m,n: a batch of one product shape instead of the mixed workload")
+    ap.add_argument("--square", action="store_true", help="with --shape: squares of m-limb operands")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

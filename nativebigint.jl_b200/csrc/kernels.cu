@@ -242,6 +242,157 @@ __device__ void round_r8(const Tiles& T, const DStage& A) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Fused middle of the last pass: the forward's last round on a and b, the
+// pointwise product and the reverse's first round (the same stages,
+// transposed) on the same registers.  The twiddles are loaded once.
+// Tiles: a_f = T.s + f * T.stride * (sq ? 1 : 2), b_f = a_f + (sq ? 0 : T.stride).
+struct FuseTiles {
+    double* s;
+    int stride;
+    int sq;
+    int G, lc, Qb, j0;
+};
+
+__device__ __forceinline__ void pw4(double* a, const double* b, Fp F) {
+#pragma unroll
+    for (int t = 0; t < 4; t++) a[t] = fp_mulmod(a[t], b[t], F);
+}
+
+template <bool FWD>
+__device__ __forceinline__ void r16_body(double* v, const double* twA, int stepA, int QA, const double* wB,
+                                         double wi, Fp F) {
+    if (FWD) {
+#pragma unroll
+        for (int t2 = 0; t2 < 4; t2++) {
+            double y[4] = {v[t2], v[4 + t2], v[8 + t2], v[12 + t2]};
+            const double w[4] = {0.0, __ldg(twA + t2 * stepA), __ldg(twA + t2 * stepA + QA),
+                                 __ldg(twA + t2 * stepA + 2 * QA)};
+            butterfly<4, true>(y, w, &wi, F);
+            v[t2] = y[0]; v[4 + t2] = y[1]; v[8 + t2] = y[2]; v[12 + t2] = y[3];
+        }
+#pragma unroll
+        for (int t1 = 0; t1 < 4; t1++) butterfly<4, true>(v + 4 * t1, wB, &wi, F);
+    } else {
+#pragma unroll
+        for (int t1 = 0; t1 < 4; t1++) butterfly<4, false>(v + 4 * t1, wB, &wi, F);
+#pragma unroll
+        for (int t2 = 0; t2 < 4; t2++) {
+            double y[4] = {v[t2], v[4 + t2], v[8 + t2], v[12 + t2]};
+            const double w[4] = {0.0, __ldg(twA + t2 * stepA), __ldg(twA + t2 * stepA + QA),
+                                 __ldg(twA + t2 * stepA + 2 * QA)};
+            butterfly<4, false>(y, w, &wi, F);
+            v[t2] = y[0]; v[4 + t2] = y[1]; v[8 + t2] = y[2]; v[12 + t2] = y[3];
+        }
+    }
+}
+
+__device__ void fused_r16(const FuseTiles& T, const DStage& A, const DStage& B) {
+    const int C = 1 << T.lc;
+    const int Lloc = (int)(A.L / T.Qb);
+    const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
+    const int QA = (int)A.Q, QB = (int)B.Q;
+    const int per = (T.G >> 4) << T.lc;
+    const int total = 2 * per;
+    const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
+    const double *twA0 = A.tw[0], *twA1 = A.tw[1], *twB0 = B.tw[0], *twB1 = B.tw[1];
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        const bool p1 = u >= per;
+        const int uu = p1 ? u - per : u;
+        const Fp F = fpctx(p1 ? 1 : 0);
+        const double wi = p1 ? wi1 : wi0;
+        double* sa = T.s + (p1 ? (T.sq ? 1 : 2) : 0) * T.stride;
+        double* sb = T.sq ? sa : sa + T.stride;
+        const int c = uu & (C - 1);
+        const int r = uu >> T.lc;
+        const int b = r >> lq, j2 = r & (q16 - 1);
+        const int row0 = b * Lloc + j2;
+#define NBG_OFF(k) sp(((row0 + ((k) >> 2) * 4 * q16 + ((k) & 3) * q16) << T.lc) + c)
+        const int jB = j2 * T.Qb + T.j0 + c;
+        const double* twB = (p1 ? twB1 : twB0) + jB;
+        const double* twA = (p1 ? twA1 : twA0) + jB;
+        const int stepA = q16 * T.Qb;
+        const double wB[4] = {0.0, __ldg(twB), __ldg(twB + QB), __ldg(twB + 2 * QB)};
+        double va[16];
+        if (!T.sq) {
+            // b's forward round goes back to its own shared slots (same thread),
+            // keeping one operand in registers at a time
+#pragma unroll
+            for (int k = 0; k < 16; k++) va[k] = sb[NBG_OFF(k)];
+            r16_body<true>(va, twA, stepA, QA, wB, wi, F);
+#pragma unroll
+            for (int k = 0; k < 16; k++) sb[NBG_OFF(k)] = va[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 16; k++) va[k] = sa[NBG_OFF(k)];
+        r16_body<true>(va, twA, stepA, QA, wB, wi, F);
+        // pointwise (fp_ntt_pointwise!, :770-785)
+        if (T.sq) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) va[k] = fp_mulmod(va[k], va[k], F);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; k++) va[k] = fp_mulmod(va[k], sb[NBG_OFF(k)], F);
+        }
+        r16_body<false>(va, twA, stepA, QA, wB, wi, F);
+#pragma unroll
+        for (int k = 0; k < 16; k++) sa[NBG_OFF(k)] = va[k];
+#undef NBG_OFF
+    }
+}
+
+__device__ void fused_r8(const FuseTiles& T, const DStage& A) {
+    const int per = T.G >> 3;
+    const int total = 2 * per;
+    const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
+    const double *tw0 = A.tw[0], *tw1 = A.tw[1];
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        const bool p1 = u >= per;
+        const int b = p1 ? u - per : u;
+        const Fp F = fpctx(p1 ? 1 : 0);
+        const double wi = p1 ? wi1 : wi0;
+        double* sa = T.s + (p1 ? (T.sq ? 1 : 2) : 0) * T.stride;
+        double* sb = T.sq ? sa : sa + T.stride;
+        const double* tw = p1 ? tw1 : tw0;
+        const double w0[4] = {0.0, __ldg(tw + 0), __ldg(tw + 2), __ldg(tw + 4)};
+        const double w1[4] = {0.0, __ldg(tw + 1), __ldg(tw + 3), __ldg(tw + 5)};
+        double va[8], vb[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) va[k] = sa[sp(8 * b + k)];
+        if (!T.sq) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) vb[k] = sb[sp(8 * b + k)];
+        }
+#pragma unroll
+        for (int op = 0; op < 2; op++) {
+            if (op == 1 && T.sq) break;
+            double* v = op ? vb : va;
+            double y[4] = {v[0], v[2], v[4], v[6]};
+            butterfly<4, true>(y, w0, &wi, F);
+            v[0] = y[0]; v[2] = y[1]; v[4] = y[2]; v[6] = y[3];
+            double z[4] = {v[1], v[3], v[5], v[7]};
+            butterfly<4, true>(z, w1, &wi, F);
+            v[1] = z[0]; v[3] = z[1]; v[5] = z[2]; v[7] = z[3];
+#pragma unroll
+            for (int i = 0; i < 4; i++) butterfly2(v[2 * i], v[2 * i + 1], F);
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) pw4(va + 4 * k, T.sq ? va + 4 * k : vb + 4 * k, F);
+#pragma unroll
+        for (int i = 0; i < 4; i++) butterfly2(va[2 * i], va[2 * i + 1], F);
+        {
+            double y[4] = {va[0], va[2], va[4], va[6]};
+            butterfly<4, false>(y, w0, &wi, F);
+            va[0] = y[0]; va[2] = y[1]; va[4] = y[2]; va[6] = y[3];
+            double z[4] = {va[1], va[3], va[5], va[7]};
+            butterfly<4, false>(z, w1, &wi, F);
+            va[1] = z[0]; va[3] = z[1]; va[5] = z[2]; va[7] = z[3];
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) sa[sp(8 * b + k)] = va[k];
+    }
+}
+
 template <bool FWD>
 __device__ void run_round(const Tiles& T, const DPlan& pl, int kind, int s0) {
     __syncthreads();
@@ -436,16 +587,37 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) k_pwr(const DProd* __restrict
             }
             cp_async_wait_all();
         }
-        run_pass<true>(make_tiles(smem, stride, sq ? 2 : 4, sq ? 0 : 1, ps, j0), pl, ps);
-        {
+        const int nr = ps.nrounds;
+        const int lastk = ps.rkind[nr - 1];
+        if (lastk == RK_R16 || lastk == RK_R8) {
+            // forward rounds but the last, fused round, reverse rounds but the first
+            const Tiles TF = make_tiles(smem, stride, sq ? 2 : 4, sq ? 0 : 1, ps, j0);
+            for (int r = 0; r < nr - 1; r++) run_round<true>(TF, pl, ps.rkind[r], ps.rstage[r]);
+            __syncthreads();
+            FuseTiles FT;
+            FT.s = smem;
+            FT.stride = stride;
+            FT.sq = sq;
+            FT.G = ps.G;
+            FT.lc = __ffs(ps.C) - 1;
+            FT.Qb = (int)ps.Qb;
+            FT.j0 = j0;
+            const int s0 = ps.rstage[nr - 1];
+            if (lastk == RK_R16) fused_r16(FT, pl.st[s0], pl.st[s0 + 1]);
+            else fused_r8(FT, pl.st[s0]);
+            const Tiles TR = make_tiles(a0, (int)(a1 - a0), 2, 0, ps, j0);
+            for (int r = nr - 2; r >= 0; r--) run_round<false>(TR, pl, ps.rkind[r], ps.rstage[r]);
+            __syncthreads();
+        } else {
+            run_pass<true>(make_tiles(smem, stride, sq ? 2 : 4, sq ? 0 : 1, ps, j0), pl, ps);
             const Fp F0 = fpctx(0), F1 = fpctx(1);
             for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
                 const int i = sp(e);
                 a0[i] = fp_mulmod(a0[i], b0[i], F0);
                 a1[i] = fp_mulmod(a1[i], b1[i], F1);
             }
+            run_pass<false>(make_tiles(a0, (int)(a1 - a0), 2, 0, ps, j0), pl, ps);
         }
-        run_pass<false>(make_tiles(a0, (int)(a1 - a0), 2, 0, ps, j0), pl, ps);
         store_tile(a0, P.xa[0], ps, base);
         store_tile(a1, P.xa[1], ps, base);
     }
@@ -489,8 +661,12 @@ __device__ __forceinline__ void garner(const double* __restrict__ x1, const doub
     v1 = v1 < 0.0 ? dadd(v1, F1.p) : v1;
     double v2 = fp_mulmod4(__ldg(x2 + idx), pl.ninv[1], pl.ninvp[1], F2);
     double u = fp_mulmod4(dsub(v2, fp_reduce(v1, F2)), c_garner[0], c_garner[1], F2);
-    uint64_t c1 = (uint64_t)v1;
-    uint64_t uu = (uint64_t)(u < 0.0 ? dadd(u, F2.p) : u);
+    u = u < 0.0 ? dadd(u, F2.p) : u;
+    // canonical values are < 2^50: adding 1.5*2^52 leaves them in the low 51
+    // mantissa bits (the reference's vector unpack does the same, :897-901)
+    const uint64_t m51 = (1ULL << 51) - 1ULL;
+    uint64_t c1 = (uint64_t)__double_as_longlong(dadd(v1, FP_MAGIC)) & m51;
+    uint64_t uu = (uint64_t)__double_as_longlong(dadd(u, FP_MAGIC)) & m51;
     // c = c1 + p1*uu  (128-bit)
     uint64_t plo = uu * P1_U;
     uint64_t phi = __umul64hi(uu, P1_U);
@@ -516,24 +692,39 @@ __device__ __forceinline__ uint32_t gp_compose(uint32_t lower, uint32_t upper) {
     return g | (p << 1);
 }
 
-// Limb value V_w = sum of slices; returns lo, sets hi (<= 4).
+// floor(x / b) for 0 <= x < 2^50 and 1 <= b <= 52: a double quotient is off
+// by at most one, fixed by an exact integer check.
+__device__ __forceinline__ int64_t fdiv_small(int64_t x, int b, double rb) {
+    int64_t q = (int64_t)__dmul_rn((double)x, rb);
+    if (q * b > x) q--;
+    else if ((q + 1) * b <= x) q++;
+    return q;
+}
+
+// Slices of the coefficients overlapping limb w, summed: returns the low 64
+// bits, sets hi (<= 4).  [i0, i1] is the coefficient range of the limb.
 __device__ __forceinline__ uint64_t limb_sum(const uint64_t* __restrict__ clo, const uint64_t* __restrict__ chi,
-                                             int64_t ibase, int64_t ilo, int64_t ihi, int b, int64_t w,
+                                             int64_t ibase, int64_t i0, int64_t i1, int b, int64_t w,
                                              uint64_t& hiout) {
-    int64_t a = 64 * w - 99;
-    int64_t i0 = a <= 0 ? 0 : (a + b - 1) / b;
-    int64_t i1 = (64 * w + 63) / b;
-    if (i0 < ilo) i0 = ilo;
-    if (i1 > ihi) i1 = ihi;
     uint64_t lo = 0, hi = 0;
-    for (int64_t i = i0; i <= i1; i++) {
-        int d = (int)(i * b - 64 * w);
+    int d = (int)(i0 * b - 64 * w);
+    for (int64_t i = i0; i <= i1; i++, d += b) {
         uint64_t sl = slice64(clo[i - ibase], chi[i - ibase], d);
         lo += sl;
         hi += (lo < sl) ? 1ULL : 0ULL;
     }
     hiout = hi;
     return lo;
+}
+
+// coefficient range [i0, i1] overlapping limb w, clamped to [ilo, ihi]
+__device__ __forceinline__ void limb_range(int64_t w, int b, double rb, int64_t ilo, int64_t ihi, int64_t& i0,
+                                           int64_t& i1) {
+    const int64_t a = 64 * w - 99;
+    i0 = a <= 0 ? 0 : fdiv_small(a + b - 1, b, rb);
+    i1 = fdiv_small(64 * w + 63, b, rb);
+    if (i0 < ilo) i0 = ilo;
+    if (i1 > ihi) i1 = ihi;
 }
 
 __global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restrict__ prods,
@@ -547,6 +738,7 @@ __global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restri
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int b = P.bch;
+        const double rb = 1.0 / (double)b;
         const int64_t N = pl.N;
         const int64_t w0 = jb.tile * UNPACK_TL;
         const int64_t w1 = min(w0 + (int64_t)UNPACK_TL, P.rn);
@@ -571,16 +763,31 @@ __global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restri
         // limb sums for this thread's LIMBS_PER_THREAD consecutive limbs
         const int t = threadIdx.x;
         uint64_t lo[LIMBS_PER_THREAD], hiv[LIMBS_PER_THREAD];
+        {
+            const int64_t wt = w0 + (int64_t)t * LIMBS_PER_THREAD;
+            int64_t i0, i1;
+            limb_range(wt, b, rb, ilo, ihi, i0, i1);
 #pragma unroll
-        for (int q = 0; q < LIMBS_PER_THREAD; q++) {
-            int64_t w = w0 + (int64_t)t * LIMBS_PER_THREAD + q;
-            if (w < w1) lo[q] = limb_sum(clo, chi, ilo, ilo, ihi, b, w, hiv[q]);
-            else { lo[q] = 0; hiv[q] = 0; }
+            for (int q = 0; q < LIMBS_PER_THREAD; q++) {
+                const int64_t w = wt + q;
+                if (q > 0) {  // advance the range by one limb (64 bits): a step or two
+                    const int64_t a = 64 * w - 99;
+                    while (i0 * b < a) i0++;
+                    if (i0 < ilo) i0 = ilo;
+                    while ((i1 + 1) * b <= 64 * w + 63 && i1 + 1 <= ihi) i1++;
+                }
+                if (w < w1) lo[q] = limb_sum(clo, chi, ilo, i0, i1, b, w, hiv[q]);
+                else { lo[q] = 0; hiv[q] = 0; }
+            }
         }
         hilast[t + 1] = hiv[LIMBS_PER_THREAD - 1];
         if (t == 0) {
             uint64_t h0 = 0;
-            if (w0 > 0) (void)limb_sum(clo, chi, ilo, ilo, ihi, b, w0 - 1, h0);
+            if (w0 > 0) {
+                int64_t i0, i1;
+                limb_range(w0 - 1, b, rb, ilo, ihi, i0, i1);
+                (void)limb_sum(clo, chi, ilo, i0, i1, b, w0 - 1, h0);
+            }
             hilast[0] = h0;
         }
         __syncthreads();

@@ -39,7 +39,8 @@ int nbg_mul(uint64_t *r, const uint64_t *a, int64_t m, const uint64_t *b, int64_
  * branch of sqr! (src/mul.jl:141-147, :134). */
 int nbg_sqr(uint64_t *r, const uint64_t *a, int64_t n);
 
-/* ---- products, device buffers (asynchronous on `stream`, a cudaStream_t) - */
+/* ---- products, device buffers (asynchronous on `stream`, a cudaStream_t; ----
+ * ---- NULL is the legacy default stream)                                  - */
 
 int nbg_mul_dev(uint64_t *r, const uint64_t *a, int64_t m, const uint64_t *b, int64_t n, void *stream);
 int nbg_sqr_dev(uint64_t *r, const uint64_t *a, int64_t n, void *stream);
@@ -142,10 +143,25 @@ int nbg_plan_info(int64_t N, int32_t *nst, int32_t *npass, int32_t *stage_m, int
 int nbg_plan_layout(int64_t N, int32_t sqr, int64_t *stages, int32_t *nst, int64_t *passes, int32_t *npass,
                     int32_t *rounds, int32_t cap);
 /* Tuning knobs (JSON object, keys: full_max_mul, full_max_sqr, last_max,
- * early_gmax, tile_target, cmax).  Changing them drops cached plans. */
+ * last_max_sqr, early_gmax, tile_target, cmax, and "overrides": a list of
+ * {"N", "sqr", "pass_ends": [last stage of each pass], "tile_target", "cmax"}
+ * giving an explicit pass split per transform class).  Changing them drops
+ * cached plans. */
 int nbg_set_tuning(const char *json);
 /* Current tuning as a JSON object into buf (NUL-terminated). */
 int nbg_get_tuning(char *buf, int64_t cap);
+/* Applies a tuning file written by the autotuner ({"gpu", "version",
+ * "tuning": {...}}) if it matches this GPU model and library version;
+ * otherwise NBG_EINVAL and the current tuning stays.  On first use the
+ * library loads $NBGPU_TUNING, else <lib dir>/../tuning/<GPU name>.json, when
+ * present and matching. */
+int nbg_load_tuning(const char *path);
+/* Frees the twiddle tables of every cached plan (including those dropped by
+ * a tuning change).  Only call it when no nbg_batch exists and no call is in
+ * flight; plans are rebuilt on demand. */
+int nbg_trim_plans(void);
+/* Library version string (tuning files are keyed by it). */
+const char *nbg_version(void);
 
 /* ---- device / errors ------------------------------------------------------ */
 

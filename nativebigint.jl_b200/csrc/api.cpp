@@ -1,8 +1,13 @@
 // api.cpp — the extern "C" entry points of include/nbgpu.h.
 #include <cuda_runtime.h>
 
+#include <dlfcn.h>
+
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/nbgpu.h"
@@ -201,7 +206,74 @@ int dev_batch(const nbg_desc* descs, int64_t count, cudaStream_t st) {
     return NBG_OK;
 }
 
-cudaStream_t as_stream(void* s) { return s ? (cudaStream_t)s : g_eng.stream; }
+// NULL is the legacy default stream, as everywhere in CUDA
+cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
+
+const char* NBG_VERSION = "0.4.0";
+
+std::string json_str(const std::string& js, const char* key) {
+    std::string k = std::string("\"") + key + "\"";
+    size_t p = js.find(k);
+    if (p == std::string::npos) return "";
+    p = js.find(':', p + k.size());
+    if (p == std::string::npos) return "";
+    p = js.find('"', p);
+    if (p == std::string::npos) return "";
+    size_t e = js.find('"', p + 1);
+    if (e == std::string::npos) return "";
+    return js.substr(p + 1, e - p - 1);
+}
+
+// Applies a tuning file written by the autotuner if it was made for this GPU
+// model and library version; anything else keeps the defaults.
+int load_tuning_file(const char* path) {
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(NBG_EINVAL, "tuning file %s not readable", path);
+    std::string js;
+    char buf[4096];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof buf, f)) > 0) js.append(buf, n);
+    fclose(f);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, g_eng.dev) != cudaSuccess) return fail(NBG_ECUDA, "device properties");
+    const std::string gpu = json_str(js, "gpu"), ver = json_str(js, "version");
+    if (gpu != prop.name || ver != NBG_VERSION)
+        return fail(NBG_EINVAL, "stale tuning file %s (gpu '%s', version '%s'; this is '%s', %s)", path, gpu.c_str(),
+                    ver.c_str(), prop.name, NBG_VERSION);
+    const size_t t = js.find("\"tuning\"");
+    if (t == std::string::npos) return fail(NBG_EINVAL, "tuning file %s has no tuning object", path);
+    const size_t ob = js.find('{', t);
+    if (ob == std::string::npos) return fail(NBG_EINVAL, "tuning file %s malformed", path);
+    int rc = g_eng.tun.from_json(js.c_str() + ob);
+    if (rc) return rc;
+    g_eng.drop_plans();
+    return NBG_OK;
+}
+
+// NBGPU_TUNING, else <library dir>/../tuning/<gpu name with spaces as _>.json
+void autoload_tuning() {
+    std::string path;
+    if (const char* env = getenv("NBGPU_TUNING")) {
+        path = env;
+    } else {
+        Dl_info info;
+        cudaDeviceProp prop;
+        if (!dladdr((void*)&autoload_tuning, &info) || !info.dli_fname) return;
+        if (cudaGetDeviceProperties(&prop, g_eng.dev) != cudaSuccess) return;
+        std::string lib = info.dli_fname;
+        size_t sl = lib.rfind('/');
+        std::string dir = sl == std::string::npos ? "." : lib.substr(0, sl);
+        std::string name = prop.name;
+        for (char& ch : name)
+            if (ch == ' ') ch = '_';
+        path = dir + "/../tuning/" + name + ".json";
+    }
+    FILE* f = fopen(path.c_str(), "rb");
+    if (!f) return;
+    fclose(f);
+    std::string keep = last_error();
+    (void)load_tuning_file(path.c_str());  // a stale or foreign file leaves the defaults
+}
 
 // One product descriptor wrapping a preloaded transform or an unpack.
 int transform_passes(double* x, int64_t N, int prime, bool fwd, cudaStream_t st) {
@@ -247,6 +319,10 @@ int transform_passes(double* x, int64_t N, int prime, bool fwd, cudaStream_t st)
 
 }  // namespace
 
+namespace nbg {
+void autoload_tuning_hook() { autoload_tuning(); }
+}  // namespace nbg
+
 // ---------------------------------------------------------------------------
 
 #define API_LOCK() std::lock_guard<std::recursive_mutex> lk_(g_eng.mu)
@@ -261,7 +337,26 @@ extern "C" {
 
 int nbg_init(int32_t device) {
     std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
-    return g_eng.init(device);
+    const bool was = g_eng.ready;
+    int rc = g_eng.init(device);
+    if (!rc && !was) autoload_tuning();
+    return rc;
+}
+
+const char* nbg_version(void) { return NBG_VERSION; }
+
+int nbg_trim_plans(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    if (g_eng.ready) g_eng.trim_plans();
+    return NBG_OK;
+}
+
+int nbg_load_tuning(const char* path) {
+    if (!path) return fail(NBG_EINVAL, "null path");
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    int rc = g_eng.ensure();
+    if (rc) return rc;
+    return load_tuning_file(path);
 }
 
 const char* nbg_last_error(void) { return last_error(); }

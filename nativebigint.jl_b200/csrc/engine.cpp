@@ -20,6 +20,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/nbgpu.h"
@@ -199,36 +200,78 @@ static int64_t pow2floor(int64_t x) {
 }
 
 std::string Tuning::to_json() const {
-    char buf[256];
+    char buf[512];
     snprintf(buf, sizeof buf,
              "{\"full_max_mul\": %d, \"full_max_sqr\": %d, \"last_max\": %d, \"last_max_sqr\": %d, "
-             "\"early_gmax\": %d, \"tile_target\": %d, \"cmax\": %d}",
+             "\"early_gmax\": %d, \"tile_target\": %d, \"cmax\": %d, \"overrides\": [",
              full_max_mul, full_max_sqr, last_max, last_max_sqr, early_gmax, tile_target, cmax);
-    return buf;
+    std::string out = buf;
+    bool first = true;
+    for (const auto& kv : overrides) {
+        out += first ? "" : ", ";
+        first = false;
+        snprintf(buf, sizeof buf, "{\"N\": %lld, \"sqr\": %d, \"tile_target\": %d, \"cmax\": %d, \"pass_ends\": [",
+                 (long long)(kv.first / 2), (int)(kv.first & 1), kv.second.tile_target, kv.second.cmax);
+        out += buf;
+        for (size_t i = 0; i < kv.second.pass_ends.size(); i++) {
+            out += (i ? ", " : "") + std::to_string(kv.second.pass_ends[i]);
+        }
+        out += "]}";
+    }
+    out += "]}";
+    return out;
 }
 
-static bool json_int(const char* js, const char* key, int* out) {
+// Minimal reader for the flat JSON objects this library writes: "key": int.
+static bool json_int(const char* js, const char* end, const char* key, long long* out) {
     std::string k = std::string("\"") + key + "\"";
-    const char* p = strstr(js, k.c_str());
-    if (!p) return false;
-    p = strchr(p + k.size(), ':');
-    if (!p) return false;
-    char* end = nullptr;
-    long v = strtol(p + 1, &end, 10);
-    if (end == p + 1) return false;
+    const char* p = js;
+    for (;;) {
+        p = strstr(p, k.c_str());
+        if (!p || p >= end) return false;
+        const char* q = p + k.size();
+        while (q < end && (*q == ' ' || *q == '\t' || *q == '\n')) q++;
+        if (q < end && *q == ':') {
+            char* e = nullptr;
+            long long v = strtoll(q + 1, &e, 10);
+            if (e == q + 1) return false;
+            *out = v;
+            return true;
+        }
+        p = q;
+    }
+}
+static bool json_int(const char* js, const char* key, int* out) {
+    long long v;
+    if (!json_int(js, js + strlen(js), key, &v)) return false;
     *out = (int)v;
     return true;
 }
 
+// matching bracket/brace end of the value starting at p (p points at '[' or '{')
+static const char* json_close(const char* p) {
+    const char open = *p, close = open == '[' ? ']' : '}';
+    int depth = 0;
+    for (; *p; p++) {
+        if (*p == open) depth++;
+        else if (*p == close && --depth == 0) return p;
+    }
+    return nullptr;
+}
+
 int Tuning::from_json(const char* js) {
     Tuning t = *this;
-    json_int(js, "full_max_mul", &t.full_max_mul);
-    json_int(js, "full_max_sqr", &t.full_max_sqr);
-    json_int(js, "last_max", &t.last_max);
-    json_int(js, "last_max_sqr", &t.last_max_sqr);
-    json_int(js, "early_gmax", &t.early_gmax);
-    json_int(js, "tile_target", &t.tile_target);
-    json_int(js, "cmax", &t.cmax);
+    // top-level scalars: read only the part before "overrides"
+    std::string head = js;
+    const char* ov = strstr(js, "\"overrides\"");
+    if (ov) head = std::string(js, ov);
+    json_int(head.c_str(), "full_max_mul", &t.full_max_mul);
+    json_int(head.c_str(), "full_max_sqr", &t.full_max_sqr);
+    json_int(head.c_str(), "last_max", &t.last_max);
+    json_int(head.c_str(), "last_max_sqr", &t.last_max_sqr);
+    json_int(head.c_str(), "early_gmax", &t.early_gmax);
+    json_int(head.c_str(), "tile_target", &t.tile_target);
+    json_int(head.c_str(), "cmax", &t.cmax);
     auto pow2 = [](int v) { return v >= 1 && (v & (v - 1)) == 0; };
     // shared memory bounds: a product's last pass holds 4 tiles (a, b per
     // prime), a square's 2; column passes hold 2 tiles of <= tile_target or G.
@@ -236,6 +279,43 @@ int Tuning::from_json(const char* js) {
         t.full_max_mul < 4 || t.full_max_sqr < 4 || t.full_max_mul > 4096 || t.full_max_sqr > 8192 ||
         t.last_max > 4096 || t.last_max_sqr > 8192 || t.early_gmax > 1024 || t.tile_target > 8192)
         return fail(NBG_EINVAL, "tuning out of range");
+    if (ov) {
+        t.overrides.clear();
+        const char* lb = strchr(ov, '[');
+        const char* le = lb ? json_close(lb) : nullptr;
+        if (!lb || !le) return fail(NBG_EINVAL, "tuning: malformed overrides");
+        const char* p = lb + 1;
+        while (p < le) {
+            const char* ob = strchr(p, '{');
+            if (!ob || ob > le) break;
+            const char* oe = json_close(ob);
+            if (!oe || oe > le) return fail(NBG_EINVAL, "tuning: malformed override");
+            long long N = 0, sq = 0, tt = 0, cm = 0;
+            if (!json_int(ob, oe, "N", &N) || N < 4) return fail(NBG_EINVAL, "tuning: override without N");
+            json_int(ob, oe, "sqr", &sq);
+            json_int(ob, oe, "tile_target", &tt);
+            json_int(ob, oe, "cmax", &cm);
+            SplitOverride so;
+            so.tile_target = (int)tt;
+            so.cmax = (int)cm;
+            if ((so.cmax && !pow2(so.cmax)) || so.tile_target < 0 || so.tile_target > 8192 || so.cmax > 1024)
+                return fail(NBG_EINVAL, "tuning: override knobs out of range");
+            const char* pe = strstr(ob, "\"pass_ends\"");
+            if (!pe || pe > oe) return fail(NBG_EINVAL, "tuning: override without pass_ends");
+            const char* ab = strchr(pe, '[');
+            const char* ae = ab ? json_close(ab) : nullptr;
+            if (!ab || !ae || ae > oe) return fail(NBG_EINVAL, "tuning: malformed pass_ends");
+            for (const char* q = ab + 1; q < ae;) {
+                char* e = nullptr;
+                long v = strtol(q, &e, 10);
+                if (e == q) { q++; continue; }
+                so.pass_ends.push_back((int)v);
+                q = e;
+            }
+            t.overrides[N * 2 + (sq ? 1 : 0)] = so;
+            p = oe + 1;
+        }
+    }
     *this = t;
     return NBG_OK;
 }
@@ -264,12 +344,16 @@ int Engine::init(int device) {
     return NBG_OK;
 }
 
+void autoload_tuning_hook();
+
 int Engine::ensure() {
     if (ready) {
         cudaSetDevice(dev);
         return NBG_OK;
     }
-    return init(0);
+    int rc = init(0);
+    if (!rc) autoload_tuning_hook();
+    return rc;
 }
 
 // Stage list, combine constants and pass split for length N (build_fp_plan,
@@ -330,9 +414,44 @@ int plan_structure(int64_t N, int for_sqr, const Tuning& tun, DPlan& d) {
         d.ninvp[f] = d.ninv[f] / P;
     }
 
-    // pass split: the last pass is the longest suffix whose span fits
-    // last_max (a contiguous block, C = 1); earlier stages are grouped
-    // greedily into column passes of at most early_gmax rows.
+    // pass split: an autotuned override for this class, else the last pass is
+    // the longest suffix whose span fits last_max (a contiguous block, C = 1)
+    // and earlier stages are grouped greedily into column passes of at most
+    // early_gmax rows.
+    const int ntiles_last = for_sqr ? 2 : 4;
+    auto ov = tun.overrides.find(N * 2 + (for_sqr ? 1 : 0));
+    if (ov != tun.overrides.end()) {
+        const SplitOverride& so = ov->second;
+        const int tt = so.tile_target ? so.tile_target : tun.tile_target;
+        const int cm = so.cmax ? so.cmax : tun.cmax;
+        const int np = (int)so.pass_ends.size();
+        if (np < 1 || np > MAXPASS || so.pass_ends.back() != S - 1)
+            return fail(NBG_EINVAL, "tuning override for N=%lld: bad pass_ends", (long long)N);
+        int sa = 0;
+        for (int p = 0; p < np; p++) {
+            const int sb = so.pass_ends[p];
+            if (sb < sa || sb >= S) return fail(NBG_EINVAL, "tuning override for N=%lld: bad pass_ends", (long long)N);
+            DPass& ps = d.pass[p];
+            ps.sa = sa;
+            ps.sb = sb;
+            ps.Qb = hs[sb].Q;
+            ps.G = (int32_t)(hs[sa].L / ps.Qb);
+            if (p == np - 1) {
+                ps.C = 1;
+                if ((size_t)ntiles_last * tile_stride_doubles(ps.G) * sizeof(double) > PASS_SMEM_LIMIT)
+                    return fail(NBG_EINVAL, "tuning override for N=%lld: last pass too large", (long long)N);
+            } else {
+                const int64_t low = ps.Qb & -ps.Qb;
+                ps.C = (int32_t)std::min<int64_t>(low, std::min<int64_t>(cm, pow2floor(std::max<int64_t>(1, tt / ps.G))));
+                if (2 * (size_t)tile_stride_doubles(ps.G * ps.C) * sizeof(double) > PASS_SMEM_LIMIT)
+                    return fail(NBG_EINVAL, "tuning override for N=%lld: column tile too large", (long long)N);
+            }
+            ps.ntiles = (N / hs[sa].L) * (ps.Qb / ps.C);
+            sa = sb + 1;
+        }
+        d.npass = np;
+        return plan_rounds(d);
+    }
     const int full_max = for_sqr ? tun.full_max_sqr : tun.full_max_mul;
     const int last_max = for_sqr ? tun.last_max_sqr : tun.last_max;
     int a = 0;
@@ -371,22 +490,27 @@ int plan_structure(int64_t N, int for_sqr, const Tuning& tun, DPlan& d) {
         ps.ntiles = N / hs[a].L;
     }
     d.npass = np;
-    // rounds: odd stages one by one; the pass's radix-4 run is paired from its
-    // smallest span upwards (radix-8 round for the span-8 stage and radix-2
-    // when the transform ends with one), a leftover radix-4 at the top alone.
-    for (int p = 0; p < np; p++) {
+    return plan_rounds(d);
+}
+
+// Rounds of every pass: odd stages one by one; the pass's radix-4 run is
+// paired from its smallest span upwards (radix-8 round for the span-8 stage
+// and radix-2 when the transform ends with one), a leftover radix-4 at the
+// top alone.
+int plan_rounds(DPlan& d) {
+    for (int p = 0; p < d.npass; p++) {
         DPass& ps = d.pass[p];
         int nr = 0;
         int s = ps.sa;
-        for (; s <= ps.sb && (hs[s].m == 3 || hs[s].m == 5 || hs[s].m == 7); s++) {
+        for (; s <= ps.sb && (d.st[s].m == 3 || d.st[s].m == 5 || d.st[s].m == 7); s++) {
             ps.rkind[nr] = RK_ODD;
             ps.rstage[nr++] = (int8_t)s;
         }
         int8_t kind[MAXST], first[MAXST];
         int nb = 0;
         int e = ps.sb;
-        if (e >= s && hs[e].m == 2) {
-            if (e - 1 >= s && hs[e - 1].m == 4 && hs[e - 1].L == 8) {
+        if (e >= s && d.st[e].m == 2) {
+            if (e - 1 >= s && d.st[e - 1].m == 4 && d.st[e - 1].L == 8) {
                 kind[nb] = RK_R8;
                 first[nb++] = (int8_t)(e - 1);
                 e -= 2;
@@ -512,6 +636,15 @@ void Engine::drop_plans() {
     plans.clear();
 }
 
+void Engine::trim_plans() {
+    cudaDeviceSynchronize();
+    for (double* t : graveyard) cudaFree(t);
+    graveyard.clear();
+    for (auto& kv : plans) cudaFree(kv.second.dtab);
+    plans.clear();
+    plan_used = 0;
+}
+
 int Engine::ensure_pool(size_t bytes) {
     if (bytes <= pool_bytes) return NBG_OK;
     if (pool) {
@@ -595,11 +728,9 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
     bb.xb_off = xb_off;
     bb.agg_off = agg_off;
 
-    std::vector<std::vector<Job>> fwd((size_t)std::max(pmax - 1, 0)), rev((size_t)std::max(pmax - 1, 0));
-    std::vector<Job> pwr, unp, car;
-    std::vector<size_t> fwd_smem(fwd.size(), 0), rev_smem(rev.size(), 0);
-    size_t pwr_smem = 0;
-
+    // Jobs of one pipeline step, grouped by kernel and shared-memory size: a
+    // launch reserves its largest job's shared memory for every CTA, so a
+    // few big-tile jobs must not lower the occupancy of the rest.
     // algorithmic FP64 instructions per butterfly of the reference schedule
     // (fwd, rev), counted on the oracle's restatement: radix-2 10, radix-3 32,
     // radix-4 40, radix-5 94/98, radix-7 173/201; pointwise 7 per point; the
@@ -613,107 +744,96 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
             default: return fwd_dir ? 173 : 201;
         }
     };
-    auto pass_ops = [&](const DPlan& pl, const DPass& ps, bool fwd_dir) {
+    auto pass_ops = [&](const DPlan& pl, const DPass& ps, bool fwd_dir) {  // per tile, one prime
         double o = 0;
         for (int s = ps.sa; s <= ps.sb; s++) o += bfly_ops(pl.st[s].m, fwd_dir) * (double)ps.G * ps.C / pl.st[s].m;
         return o;
     };
-    std::vector<double> fwd_ops(fwd.size(), 0), fwd_bytes(fwd.size(), 0), rev_ops(fwd.size(), 0),
-        rev_bytes(fwd.size(), 0);
-    double pwr_ops = 0, pwr_bytes = 0, unp_ops = 0, unp_bytes = 0;
-    for (int64_t k = 0; k < count; k++) {
-        const DProd& P = bb.prods[(size_t)k];
-        const DPlan& pl = bb.plan_of[(size_t)k]->d;
-        const int Pn = P.npass;
-        const double N = (double)pl.N;
-        const double ops_cnt = P.sqr ? 1.0 : 2.0;
-        for (int p = 0; p < Pn - 1; p++) {
-            const DPass& ps = pl.pass[p];
-            const size_t step = (size_t)(pmax - Pn + p);
-            fwd_ops[step] += 2.0 * ops_cnt * pass_ops(pl, ps, true) * (double)ps.ntiles;
-            const double in_b = p == 0 ? (double)(P.nca + (P.sqr ? 0 : P.ncb)) * P.bch / 8.0
-                                       : 2.0 * ops_cnt * 8.0 * N;
-            fwd_bytes[step] += in_b + 2.0 * ops_cnt * 8.0 * N;
-        }
-        {
-            const DPass& ps = pl.pass[Pn - 1];
-            pwr_ops += 2.0 * (ops_cnt * pass_ops(pl, ps, true) + 7.0 * ps.G + pass_ops(pl, ps, false)) *
-                       (double)ps.ntiles;
-            const double in_b = Pn == 1 ? (double)(P.nca + (P.sqr ? 0 : P.ncb)) * P.bch / 8.0
-                                        : 2.0 * ops_cnt * 8.0 * N;
-            pwr_bytes += in_b + 2.0 * 8.0 * N;
-        }
-        for (int p = Pn - 2; p >= 0; p--) {
-            const size_t step = (size_t)(Pn - 2 - p);
-            rev_ops[step] += 2.0 * pass_ops(pl, pl.pass[p], false) * (double)pl.pass[p].ntiles;
-            rev_bytes[step] += 2.0 * 16.0 * N;
-        }
-        unp_ops += 28.0 * (double)P.nconv;
-        unp_bytes += 16.0 * (double)P.nconv + 8.0 * (double)P.rn;
-    }
-
-    // jobs per step (alignment: every product's pointwise pass runs in one launch);
-    // each pass job covers one tile of both primes
-    for (int64_t k = 0; k < count; k++) {
-        const DProd& P = bb.prods[(size_t)k];
-        const DPlan& pl = bb.plan_of[(size_t)k]->d;
-        const int Pn = P.npass;
-        for (int p = 0; p < Pn - 1; p++) {
-            const DPass& ps = pl.pass[p];
-            const size_t step = (size_t)(pmax - Pn + p);
-            for (int op = 0; op < (P.sqr ? 1 : 2); op++)
-                for (int64_t t = 0; t < ps.ntiles; t++) fwd[step].push_back(Job{(int32_t)k, (op << 1) | (p << 8), t});
-            fwd_smem[step] = std::max(fwd_smem[step], sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C));
-        }
-        {
-            const DPass& ps = pl.pass[Pn - 1];
-            for (int64_t t = 0; t < ps.ntiles; t++) pwr.push_back(Job{(int32_t)k, (Pn - 1) << 8, t});
-            pwr_smem = std::max(pwr_smem, sizeof(double) * (P.sqr ? 2 : 4) * (size_t)tile_stride_doubles(ps.G * ps.C));
-        }
-        for (int p = Pn - 2; p >= 0; p--) {
-            const DPass& ps = pl.pass[p];
-            const size_t step = (size_t)(Pn - 2 - p);
-            for (int64_t t = 0; t < ps.ntiles; t++) rev[step].push_back(Job{(int32_t)k, p << 8, t});
-            rev_smem[step] = std::max(rev_smem[step], sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C));
-        }
-        for (int64_t t = 0; t < P.ntl; t++) unp.push_back(Job{(int32_t)k, 0, t});
-        if (P.ntl > 1) car.push_back(Job{(int32_t)k, 0, 0});
-    }
-    // Order jobs so CTAs that run together share twiddle columns: by plan
-    // (transform length), then tile, then product.  Every product of one
-    // length reads the same twiddle slice for the same tile, so the slice is
-    // fetched from DRAM once and served from L2 to the rest.  Biggest plans
-    // first so the tail of each launch is short.
-    auto by_plan_tile = [&](std::vector<Job>& v) {
-        std::stable_sort(v.begin(), v.end(), [&](const Job& x, const Job& y) {
-            const DPlan& px = bb.plan_of[(size_t)x.prod]->d;
-            const DPlan& py = bb.plan_of[(size_t)y.prod]->d;
-            if (px.N != py.N) return px.N > py.N;
-            const int sx = bb.prods[(size_t)x.prod].plan, sy = bb.prods[(size_t)y.prod].plan;
-            if (sx != sy) return sx < sy;
-            if (x.tile != y.tile) return x.tile < y.tile;
-            return x.sub < y.sub;
-        });
+    struct Group {
+        std::vector<Job> jobs;
+        double ops = 0, bytes = 0;
     };
-    for (auto& v : fwd) by_plan_tile(v);
-    for (auto& v : rev) by_plan_tile(v);
-    by_plan_tile(pwr);
-    auto add = [&](int kind, std::vector<Job>& v, size_t smem, double ops, double bytes) {
-        if (v.empty()) return;
-        Launch L{kind, (int64_t)bb.jobs.size(), (int64_t)v.size(), smem};
-        L.alg_ops = ops;
-        L.alg_bytes = bytes;
+    // key: (step order, kind, smem)
+    std::map<std::tuple<int, int, size_t>, Group> groups;
+    auto add_job = [&](int order, int kind, size_t smem, const Job& j, double ops, double bytes) {
+        Group& g = groups[std::make_tuple(order, kind, smem)];
+        g.jobs.push_back(j);
+        g.ops += ops;
+        g.bytes += bytes;
+    };
+    // step order: forward steps 0..pmax-2, the pointwise step pmax-1, reverse
+    // steps pmax..2pmax-2, unpack 2pmax-1, carry 2pmax
+    for (int64_t k = 0; k < count; k++) {
+        const DProd& P = bb.prods[(size_t)k];
+        const DPlan& pl = bb.plan_of[(size_t)k]->d;
+        const int Pn = P.npass;
+        const double nops = P.sqr ? 1.0 : 2.0;
+        for (int p = 0; p < Pn - 1; p++) {
+            const DPass& ps = pl.pass[p];
+            const size_t smem = sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
+            const double pts = (double)ps.G * ps.C;
+            const double ops = 2.0 * pass_ops(pl, ps, true);
+            for (int op = 0; op < (P.sqr ? 1 : 2); op++) {
+                const double in_b = p == 0 ? pts * P.bch / 8.0 : 2.0 * 8.0 * pts;
+                for (int64_t t = 0; t < ps.ntiles; t++)
+                    add_job(pmax - Pn + p, JK_FWD, smem, Job{(int32_t)k, (op << 1) | (p << 8), t}, ops,
+                            in_b + 2.0 * 8.0 * pts);
+            }
+        }
+        {
+            const DPass& ps = pl.pass[Pn - 1];
+            const size_t smem = sizeof(double) * (P.sqr ? 2 : 4) * (size_t)tile_stride_doubles(ps.G * ps.C);
+            const double pts = (double)ps.G * ps.C;
+            const double ops = 2.0 * (nops * pass_ops(pl, ps, true) + 7.0 * pts + pass_ops(pl, ps, false));
+            const double in_b = Pn == 1 ? nops * pts * P.bch / 8.0 : 2.0 * nops * 8.0 * pts;
+            for (int64_t t = 0; t < ps.ntiles; t++)
+                add_job(pmax - 1, JK_PWR, smem, Job{(int32_t)k, (Pn - 1) << 8, t}, ops, in_b + 2.0 * 8.0 * pts);
+        }
+        for (int p = Pn - 2; p >= 0; p--) {
+            const DPass& ps = pl.pass[p];
+            const size_t smem = sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
+            const double pts = (double)ps.G * ps.C;
+            for (int64_t t = 0; t < ps.ntiles; t++)
+                add_job(pmax + (Pn - 2 - p), JK_REV, smem, Job{(int32_t)k, p << 8, t}, 2.0 * pass_ops(pl, ps, false),
+                        2.0 * 16.0 * pts);
+        }
+    }
+    const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / bmin + 4;
+    const size_t unp_smem = sizeof(uint64_t) * 2 * (size_t)align_up((size_t)ncoef, 2);
+    for (int64_t k = 0; k < count; k++) {
+        const DProd& P = bb.prods[(size_t)k];
+        const double per_tile_ops = 28.0 * (double)P.nconv / (double)P.ntl;
+        const double per_tile_bytes = (16.0 * (double)P.nconv + 8.0 * (double)P.rn) / (double)P.ntl;
+        for (int64_t t = 0; t < P.ntl; t++)
+            add_job(2 * pmax - 1, JK_UNPACK, unp_smem, Job{(int32_t)k, 0, t}, per_tile_ops, per_tile_bytes);
+        if (P.ntl > 1) add_job(2 * pmax, JK_CARRY, 0, Job{(int32_t)k, 0, 0}, 0.0, 4.0 * (double)P.ntl);
+    }
+    // Within a launch: jobs ordered so CTAs that run together share twiddle
+    // columns — by plan (transform length), then tile, then product.  Every
+    // product of one length reads the same twiddle slice for the same tile, so
+    // the slice comes from DRAM once and from L2 for the rest.  Biggest plans
+    // first so the tail of each launch is short.
+    for (auto& kv : groups) {
+        const int kind = std::get<1>(kv.first);
+        std::vector<Job>& v = kv.second.jobs;
+        if (kind == JK_FWD || kind == JK_REV || kind == JK_PWR) {
+            std::stable_sort(v.begin(), v.end(), [&](const Job& x, const Job& y) {
+                const DPlan& px = bb.plan_of[(size_t)x.prod]->d;
+                const DPlan& py = bb.plan_of[(size_t)y.prod]->d;
+                if (px.N != py.N) return px.N > py.N;
+                const int sx = bb.prods[(size_t)x.prod].plan, sy = bb.prods[(size_t)y.prod].plan;
+                if (sx != sy) return sx < sy;
+                if (x.tile != y.tile) return x.tile < y.tile;
+                return x.sub < y.sub;
+            });
+        }
+        Launch L{kind, (int64_t)bb.jobs.size(), (int64_t)v.size(), std::get<2>(kv.first)};
+        L.alg_ops = kv.second.ops;
+        L.alg_bytes = kv.second.bytes;
+        if ((int)L.smem > E.smem_optin) return fail(NBG_EINVAL, "tile needs %zu bytes of shared memory", L.smem);
         bb.launches.push_back(L);
         bb.jobs.insert(bb.jobs.end(), v.begin(), v.end());
-    };
-    for (size_t s = 0; s < fwd.size(); s++) add(JK_FWD, fwd[s], fwd_smem[s], fwd_ops[s], fwd_bytes[s]);
-    add(JK_PWR, pwr, pwr_smem, pwr_ops, pwr_bytes);
-    for (size_t s = 0; s < rev.size(); s++) add(JK_REV, rev[s], rev_smem[s], rev_ops[s], rev_bytes[s]);
-    const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / bmin + 4;
-    add(JK_UNPACK, unp, sizeof(uint64_t) * 2 * (size_t)align_up((size_t)ncoef, 2), unp_ops, unp_bytes);
-    add(JK_CARRY, car, 0, 0.0, 4.0 * (double)car.size());
-    for (const Launch& L : bb.launches)
-        if ((int)L.smem > E.smem_optin) return fail(NBG_EINVAL, "tile needs %zu bytes of shared memory", L.smem);
+    }
 
     // device layout: [prods | jobs | work | agg]
     bb.off_prods = 0;

@@ -21,6 +21,14 @@ int64_t magnitude_bits(const uint64_t* a, int64_t n);
 int64_t ntt_len(int64_t T);
 int ntt_params(int64_t bits_a, int64_t bits_b, int* b_out, int64_t* N_out);
 
+// An explicit pass split for one (transform length, square) class, chosen by
+// the autotuner: the last stage of each pass, and the column-tile knobs.
+struct SplitOverride {
+    std::vector<int> pass_ends;
+    int tile_target = 0;  // 0: the global value
+    int cmax = 0;
+};
+
 // Pass-split knobs (the autotuner's search space).
 struct Tuning {
     int full_max_mul = 2048;  // one-pass (whole transform in shared memory) up to this N, products
@@ -30,11 +38,16 @@ struct Tuning {
     int early_gmax = 256;     // largest row count of an early (column) pass
     int tile_target = 2048;   // target doubles per column-pass tile
     int cmax = 128;           // most adjacent columns per column-pass tile
+    std::map<int64_t, SplitOverride> overrides;  // key: N * 2 + square
     std::string to_json() const;
     int from_json(const char* js);
 };
 
+// shared memory the pass kernels may use per CTA (B200 opt-in is 227 KB)
+constexpr size_t PASS_SMEM_LIMIT = 220 * 1024;
+
 int plan_structure(int64_t N, int for_sqr, const Tuning& tun, DPlan& d);
+int plan_rounds(DPlan& d);
 
 struct PlanRec {
     DPlan d;
@@ -64,6 +77,7 @@ struct Engine {
     int build_plan(int64_t N, PlanRec& pr, int for_sqr);
     int get_plan(int64_t N, int for_sqr, PlanRec** out);
     void drop_plans();
+    void trim_plans();  // frees every plan's tables: no batch may exist or be running
     int ensure_pool(size_t bytes);
 };
 extern Engine g_eng;

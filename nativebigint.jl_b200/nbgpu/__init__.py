@@ -35,7 +35,7 @@ EXPORTS = [
     "nbg_ntt_params", "nbg_ntt_len", "nbg_magnitude_bits", "nbg_pack_dev", "nbg_ntt_fwd_dev",
     "nbg_ntt_rev_dev", "nbg_pointwise_dev", "nbg_unpack_dev", "nbg_plan_info", "nbg_plan_layout", "nbg_set_tuning",
     "nbg_get_tuning", "nbg_init", "nbg_last_error", "nbg_default_stream", "nbg_launch_count",
-    "nbg_mul_dev_noalloc",
+    "nbg_mul_dev_noalloc", "nbg_load_tuning", "nbg_version", "nbg_trim_plans",
 ]
 
 
@@ -93,6 +93,7 @@ def lib() -> ctypes.CDLL:
             "nbg_set_tuning": [c.c_char_p],
             "nbg_get_tuning": [c.c_char_p, i64],
             "nbg_init": [i32],
+            "nbg_load_tuning": [c.c_char_p],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -104,6 +105,10 @@ def lib() -> ctypes.CDLL:
         L.nbg_last_error.restype = c.c_char_p
         L.nbg_default_stream.argtypes = []
         L.nbg_default_stream.restype = vp
+        L.nbg_trim_plans.argtypes = []
+        L.nbg_trim_plans.restype = c.c_int
+        L.nbg_version.argtypes = []
+        L.nbg_version.restype = c.c_char_p
         L.nbg_launch_count.argtypes = []
         L.nbg_launch_count.restype = i64
         _lib = L
@@ -349,9 +354,22 @@ def set_tuning(js: str) -> None:
 
 
 def get_tuning() -> str:
-    buf = ctypes.create_string_buffer(512)
-    _check(lib().nbg_get_tuning(buf, 512))
+    buf = ctypes.create_string_buffer(1 << 16)
+    _check(lib().nbg_get_tuning(buf, 1 << 16))
     return buf.value.decode()
+
+
+def load_tuning(path: str) -> None:
+    _check(lib().nbg_load_tuning(path.encode()))
+
+
+def trim_plans() -> None:
+    """Frees cached plans' device tables (no Batch may be alive)."""
+    _check(lib().nbg_trim_plans())
+
+
+def version() -> str:
+    return lib().nbg_version().decode()
 
 
 def launch_count() -> int:

@@ -115,7 +115,7 @@ def _emulate_plan(N, layout):
     stages, passes, rounds = layout["stages"], layout["passes"], layout["rounds"]
     seen = {s: [] for s in range(len(stages))}
     for (sa, sb, G, C, Qb, ntiles), rds in zip(passes, rounds):
-        assert C & (C - 1) == 0 and Qb % C == 0 and G * C <= 8192
+        assert C & (C - 1) == 0 and Qb % C == 0 and 2 * _stride(G * C) * 8 <= 220 * 1024
         La = stages[sa][1]
         assert La % Qb == 0 and La // Qb == G
         per = Qb // C
@@ -266,3 +266,24 @@ def test_unpack_tile_coefficient_ranges():
                 lo_i = max(0, -(-(64 * w - 99) // b))
                 hi_i = (64 * w + 63) // b
                 assert lo_i >= ilo and min(hi_i, nconv - 1) <= ihi
+
+
+def test_autotune_candidates_emulate_cleanly():
+    # every split the autotuner may time is a valid plan whose kernels stay in bounds
+    import json
+
+    from nbgpu import autotune
+
+    old = nbgpu.get_tuning()
+    try:
+        for N, sq in ((2048, False), (4096, True), (6144, False), (12288, True), (24576, False),
+                      (105 * 2**11, False), (7 * 2**15, True), (315 * 2**10, False)):
+            for cand in autotune.candidates(N, sq):
+                base = json.loads(old)
+                base["overrides"] = [dict(cand, N=N, sqr=int(sq))]
+                nbgpu.set_tuning(json.dumps(base))
+                lay = nbgpu.plan_layout(N, sq)
+                assert [p[1] for p in lay["passes"]] == cand["pass_ends"]
+                _emulate_plan(N, lay)
+    finally:
+        nbgpu.set_tuning(old)

@@ -26,6 +26,24 @@
 #include "butterfly.cuh"
 #include "kernels.h"
 
+// Minimum resident CTAs per SM the pass kernels are compiled for (register
+// budget 65536 / (256 * minb) = 80 at 3).  Measured on B200 with the mixed
+// 10,000-product batch: 3 CTAs/SM beats 2 by 10% (column passes by 20%)
+// despite a few spills; 1 CTA/SM is 35% slower.
+#ifndef NBG_PWR_MINB
+#define NBG_PWR_MINB 3
+#endif
+#ifndef NBG_COL_MINB
+#define NBG_COL_MINB 3
+#endif
+// Rounds are inlined into the kernels; out-of-line rounds (NBG_ROUND_NOINLINE)
+// measured 40% slower in k_pwr.
+#ifdef NBG_ROUND_NOINLINE
+#define NBG_ROUND __noinline__
+#else
+#define NBG_ROUND
+#endif
+
 namespace nbg {
 
 __constant__ Fp c_fp[2];
@@ -82,7 +100,7 @@ __device__ __forceinline__ int split_unit(int u, int per, int& tau) {
 
 // Generic stage: one butterfly per unit, any radix (odd stages, lone radix-4/2).
 template <int M, bool FWD>
-__device__ void round_gen(const Tiles& T, const DStage& st) {
+__device__ NBG_ROUND void round_gen(const Tiles& T, const DStage& st) {
     const int C = 1 << T.lc;
     const int Lloc = (int)(st.L / T.Qb), Qloc = (int)(st.Q / T.Qb);
     const int Q = (int)st.Q;
@@ -138,7 +156,7 @@ __device__ void round_gen(const Tiles& T, const DStage& st) {
 // Forward: A's butterflies run over t1 for each t2 (column j2 + t2*L/16), then
 // B's over t2 for each t1 (column j2).  Reverse: B then A, transposed.
 template <bool FWD>
-__device__ void round_r16(const Tiles& T, const DStage& A, const DStage& B) {
+__device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStage& B) {
     const int C = 1 << T.lc;
     const int Lloc = (int)(A.L / T.Qb);
     const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
@@ -202,7 +220,7 @@ __device__ void round_r16(const Tiles& T, const DStage& A, const DStage& B) {
 // Radix-8 round: the span-8 radix-4 stage A (Q = 2) and the radix-2 stage, on
 // 8 consecutive points (contiguous passes only: C = 1, Qb = 1, j0 = 0).
 template <bool FWD>
-__device__ void round_r8(const Tiles& T, const DStage& A) {
+__device__ NBG_ROUND void round_r8(const Tiles& T, const DStage& A) {
     const int per = T.G >> 3;
     const int total = per * T.ntiles;
     const Fp F0 = fpctx(0), F1 = fpctx(1);
@@ -287,7 +305,7 @@ __device__ __forceinline__ void r16_body(double* v, const double* twA, int stepA
     }
 }
 
-__device__ void fused_r16(const FuseTiles& T, const DStage& A, const DStage& B) {
+__device__ NBG_ROUND void fused_r16(const FuseTiles& T, const DStage& A, const DStage& B) {
     const int C = 1 << T.lc;
     const int Lloc = (int)(A.L / T.Qb);
     const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
@@ -341,7 +359,7 @@ __device__ void fused_r16(const FuseTiles& T, const DStage& A, const DStage& B) 
     }
 }
 
-__device__ void fused_r8(const FuseTiles& T, const DStage& A) {
+__device__ NBG_ROUND void fused_r8(const FuseTiles& T, const DStage& A) {
     const int per = T.G >> 3;
     const int total = 2 * per;
     const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
@@ -521,7 +539,7 @@ __device__ __forceinline__ Tiles make_tiles(double* s, int stride, int ntiles, i
 
 // ---------------------------------------------------------------------------
 // Forward pass of one tile of one operand, both primes (tiles X0, X1).
-__global__ void __launch_bounds__(PASS_THREADS, 2) k_fwd(const DProd* __restrict__ prods,
+__global__ void __launch_bounds__(PASS_THREADS, NBG_COL_MINB) k_fwd(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];
@@ -555,7 +573,7 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) k_fwd(const DProd* __restrict
 
 // Last pass, both primes: forward on a (and b), pointwise, reverse on a.
 // Tiles: products [a0, b0, a1, b1], squares [a0, a1].
-__global__ void __launch_bounds__(PASS_THREADS, 2) k_pwr(const DProd* __restrict__ prods,
+__global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];
@@ -624,7 +642,7 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) k_pwr(const DProd* __restrict
 }
 
 // Reverse pass of one tile, both primes.
-__global__ void __launch_bounds__(PASS_THREADS, 2) k_rev(const DProd* __restrict__ prods,
+__global__ void __launch_bounds__(PASS_THREADS, NBG_COL_MINB) k_rev(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];

@@ -19,7 +19,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libnbgpu.so")
+LIB_PATH = os.environ.get("NBGPU_LIB") or os.path.join(os.path.dirname(_HERE), "lib", "libnbgpu.so")
 
 NBG_OK, NBG_EINVAL, NBG_ERANGE, NBG_ENOMEM, NBG_ECUDA, NBG_ETIMEOUT, NBG_EBUSY, NBG_ENODEV = range(8)
 

@@ -80,7 +80,10 @@ typedef struct nbg_desc {
 } nbg_desc;
 
 /* Whole batch in one call, host buffers, synchronous.  Products of any size
- * run together in one launch per pipeline step. */
+ * run together in one launch per pipeline step; the batch is cut into chunks
+ * whose copies overlap the neighbouring chunks' products.  Results must not
+ * overlap any operand of the batch.  Pinned (page-locked) buffers get
+ * asynchronous DMA; contiguous operands are copied together. */
 int nbg_mul_batch(const nbg_desc *descs, int64_t count);
 
 /* Same with device buffers, asynchronous on `stream`. */

@@ -58,24 +58,58 @@ int check_desc(const nbg_desc& d, ProdIn& q, bool host) {
     return NBG_OK;
 }
 
-// pinned host staging for the host-buffer calls
-void* g_hpin = nullptr;
-size_t g_hpin_bytes = 0;
-int ensure_hpin(size_t bytes) {
-    if (bytes <= g_hpin_bytes) return NBG_OK;
-    if (g_hpin) cudaFreeHost(g_hpin);
-    g_hpin = nullptr;
-    g_hpin_bytes = 0;
-    size_t want = std::max(bytes, (size_t)16 << 20);
-    if (cudaHostAlloc(&g_hpin, want, cudaHostAllocDefault) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(NBG_ENOMEM, "pinned staging of %zu bytes unavailable", want);
+namespace {
+
+constexpr size_t CHUNK_BYTES = size_t(64) << 20;
+constexpr int NBUF = 2;
+
+struct Span {
+    const char* h;  // host start
+    size_t n;       // bytes
+    size_t d;       // offset in the chunk's span area
+};
+
+// Merges [p, p + n) ranges into spans; `gap` bytes of slack may be bridged.
+// Returns for each range its device offset; spans[] gets the copies.
+size_t layout_spans(const std::vector<std::pair<const char*, size_t>>& rg, size_t gap, std::vector<Span>& spans,
+                    std::vector<size_t>& dev_off) {
+    std::vector<size_t> ord(rg.size());
+    for (size_t i = 0; i < ord.size(); i++) ord[i] = i;
+    std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return rg[x].first < rg[y].first; });
+    dev_off.assign(rg.size(), 0);
+    spans.clear();
+    size_t total = 0;
+    for (size_t k = 0; k < ord.size(); k++) {
+        const char* p = rg[ord[k]].first;
+        const size_t n = rg[ord[k]].second;
+        if (!spans.empty()) {
+            Span& sp = spans.back();
+            const char* end = sp.h + sp.n;
+            if (p >= sp.h && p <= end + gap) {  // extend the span
+                const char* ne = std::max(end, p + n);
+                total += (size_t)(ne - end);
+                sp.n = (size_t)(ne - sp.h);
+                dev_off[ord[k]] = sp.d + (size_t)(p - sp.h);
+                continue;
+            }
+        }
+        total = align_up(total, 256);
+        spans.push_back(Span{p, n, total});
+        dev_off[ord[k]] = total;
+        total += n;
     }
-    g_hpin_bytes = want;
-    return NBG_OK;
+    return align_up(total, 256);
 }
 
-// Host-buffer batch: stage operands in pinned memory, one copy each way.
+struct Chunk {
+    int64_t start, count;
+    BatchBuild bb;
+    std::vector<Span> in_spans, out_spans;
+    size_t in_bytes = 0, out_bytes = 0, region = 0;
+};
+
+}  // namespace
+
 int host_batch(const nbg_desc* descs, int64_t count) {
     if (!descs || count <= 0) return fail(NBG_EINVAL, "empty batch");
     Engine& E = g_eng;
@@ -88,56 +122,106 @@ int host_batch(const nbg_desc* descs, int64_t count) {
         int rc = E.ensure();
         if (rc) return rc;
     }
-    // operand/result layout in the staging area
-    std::vector<size_t> oa((size_t)count), ob((size_t)count), orr((size_t)count);
-    size_t ops = 0;
-    for (int64_t k = 0; k < count; k++) {
-        const ProdIn& q = in[(size_t)k];
-        oa[(size_t)k] = ops;
-        ops = align_up(ops + 8 * (size_t)q.m, 256);
-        if (!q.sqr) {
-            ob[(size_t)k] = ops;
-            ops = align_up(ops + 8 * (size_t)q.n, 256);
+    // chunks of ~CHUNK_BYTES operands, in input order
+    std::vector<Chunk> chunks;
+    {
+        size_t acc = 0;
+        int64_t st = 0;
+        for (int64_t k = 0; k < count; k++) {
+            const ProdIn& q = in[(size_t)k];
+            acc += 8 * (size_t)(q.m + (q.sqr ? 0 : q.n));
+            if (acc >= CHUNK_BYTES || k == count - 1) {
+                Chunk c;
+                c.start = st;
+                c.count = k + 1 - st;
+                chunks.push_back(std::move(c));
+                st = k + 1;
+                acc = 0;
+            }
         }
     }
-    const size_t in_bytes = ops;
-    for (int64_t k = 0; k < count; k++) {
-        orr[(size_t)k] = ops;
-        ops = align_up(ops + 8 * (size_t)(in[(size_t)k].m + in[(size_t)k].n), 256);
+    size_t region = 0;
+    for (Chunk& c : chunks) {
+        int rc = build_batch(E, in.data() + c.start, c.count, c.bb);
+        if (rc) return rc;
+        std::vector<std::pair<const char*, size_t>> ir, orr;
+        for (int64_t k = 0; k < c.count; k++) {
+            const ProdIn& q = in[(size_t)(c.start + k)];
+            ir.push_back({(const char*)q.a, 8 * (size_t)q.m});
+            if (!q.sqr) ir.push_back({(const char*)q.b, 8 * (size_t)q.n});
+            orr.push_back({(const char*)q.r, 8 * (size_t)(q.m + q.n)});
+        }
+        std::vector<size_t> ioff, ooff;
+        c.in_bytes = layout_spans(ir, 0, c.in_spans, ioff);
+        c.out_bytes = layout_spans(orr, 0, c.out_spans, ooff);
+        const size_t base_in = align_up(c.bb.dev_bytes, 256), base_out = base_in + c.in_bytes;
+        size_t ii = 0;
+        for (int64_t k = 0; k < c.count; k++) {
+            const ProdIn& q = in[(size_t)(c.start + k)];
+            DProd& P = c.bb.prods[(size_t)k];
+            // device addresses are relative to the region; made absolute below
+            P.a = (const uint64_t*)(uintptr_t)(base_in + ioff[ii++]);
+            P.b = q.sqr ? P.a : (const uint64_t*)(uintptr_t)(base_in + ioff[ii++]);
+            P.r = (uint64_t*)(uintptr_t)(base_out + ooff[(size_t)k]);
+        }
+        c.region = align_up(base_out + c.out_bytes, 256);
+        region = std::max(region, c.region);
     }
-    const size_t out_bytes = ops - in_bytes;
-    BatchBuild bb;
-    int rc = build_batch(E, in.data(), count, bb);
+    const int nbuf = std::min<int>(NBUF, (int)chunks.size());
+    int rc = E.ensure_pool(region * (size_t)nbuf);
     if (rc) return rc;
-    const size_t dev_ops = align_up(bb.dev_bytes, 256);
-    rc = E.ensure_pool(dev_ops + ops);
-    if (rc) return rc;
-    rc = ensure_hpin(ops);
-    if (rc) return rc;
-    char* dbase = (char*)E.pool;
-    char* dop = dbase + dev_ops;
-    char* hp = (char*)g_hpin;
-    for (int64_t k = 0; k < count; k++) {
-        const ProdIn& q = in[(size_t)k];
-        memcpy(hp + oa[(size_t)k], q.a, 8 * (size_t)q.m);
-        if (!q.sqr) memcpy(hp + ob[(size_t)k], q.b, 8 * (size_t)q.n);
-        DProd& P = bb.prods[(size_t)k];
-        P.a = (const uint64_t*)(dop + oa[(size_t)k]);
-        P.b = q.sqr ? P.a : (const uint64_t*)(dop + ob[(size_t)k]);
-        P.r = (uint64_t*)(dop + orr[(size_t)k]);
+    cudaEvent_t ev_in[NBUF], ev_comp[NBUF], ev_out[NBUF];
+    for (int i = 0; i < NBUF; i++) {
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_comp[i], cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_out[i], cudaEventDisableTiming));
     }
-    cudaStream_t st = E.stream;
-    CUDA_TRY(cudaMemcpyAsync(dop, hp, in_bytes, cudaMemcpyHostToDevice, st));
-    rc = upload_batch(E, bb, dbase, st);
-    if (rc) return rc;
-    rc = run_launches(E, bb, dbase, st);
-    if (rc) return rc;
-    CUDA_TRY(cudaMemcpyAsync(hp + in_bytes, dop + in_bytes, out_bytes, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    for (int64_t k = 0; k < count; k++) {
-        const ProdIn& q = in[(size_t)k];
-        memcpy(q.r, hp + orr[(size_t)k], 8 * (size_t)(q.m + q.n));
+    for (size_t ci = 0; ci < chunks.size() && rc == NBG_OK; ci++) {
+        Chunk& c = chunks[ci];
+        const int buf = (int)(ci % (size_t)nbuf);
+        char* base = (char*)E.pool + (size_t)buf * region;
+        for (DProd& P : c.bb.prods) {
+            P.a = (const uint64_t*)(base + (uintptr_t)P.a);
+            P.b = (const uint64_t*)(base + (uintptr_t)P.b);
+            P.r = (uint64_t*)(base + (uintptr_t)P.r);
+        }
+        if (ci >= (size_t)nbuf) {  // the region's previous chunk must be fully drained
+            if (cudaStreamWaitEvent(E.copy_in, ev_out[buf], 0) != cudaSuccess) { rc = fail(NBG_ECUDA, "wait"); break; }
+        }
+        const size_t base_in = align_up(c.bb.dev_bytes, 256);
+        if ((rc = upload_batch(E, c.bb, base, E.copy_in))) break;
+        for (const Span& sp : c.in_spans)
+            if (cudaMemcpyAsync(base + base_in + sp.d, sp.h, sp.n, cudaMemcpyHostToDevice, E.copy_in) != cudaSuccess) {
+                rc = fail(NBG_ECUDA, "operand copy failed");
+                break;
+            }
+        if (rc) break;
+        cudaEventRecord(ev_in[buf], E.copy_in);
+        cudaStreamWaitEvent(E.stream, ev_in[buf], 0);
+        if ((rc = run_launches(E, c.bb, base, E.stream))) break;
+        cudaEventRecord(ev_comp[buf], E.stream);
+        cudaStreamWaitEvent(E.copy_out, ev_comp[buf], 0);
+        const size_t base_out = base_in + c.in_bytes;
+        for (const Span& sp : c.out_spans)
+            if (cudaMemcpyAsync((void*)sp.h, base + base_out + sp.d, sp.n, cudaMemcpyDeviceToHost, E.copy_out) !=
+                cudaSuccess) {
+                rc = fail(NBG_ECUDA, "result copy failed");
+                break;
+            }
+        if (rc) break;
+        cudaEventRecord(ev_out[buf], E.copy_out);
     }
+    cudaError_t e1 = cudaStreamSynchronize(E.copy_in);
+    cudaError_t e2 = cudaStreamSynchronize(E.stream);
+    cudaError_t e3 = cudaStreamSynchronize(E.copy_out);
+    for (int i = 0; i < NBUF; i++) {
+        cudaEventDestroy(ev_in[i]);
+        cudaEventDestroy(ev_comp[i]);
+        cudaEventDestroy(ev_out[i]);
+    }
+    if (rc) return rc;
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+        return fail(NBG_ECUDA, "host batch: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3));
     return NBG_OK;
 }
 

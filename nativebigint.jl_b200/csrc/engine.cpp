@@ -335,6 +335,8 @@ int Engine::init(int device) {
     if (device < 0 || device >= ndev) return fail(NBG_EINVAL, "device %d out of range", device);
     CUDA_TRY(cudaSetDevice(device));
     CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&copy_in, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&copy_out, cudaStreamNonBlocking));
     CUDA_TRY(kernels_init((double)PR[0], (double)PR[1]));
     CUDA_TRY(cudaMalloc(&d_plans, sizeof(DPlan) * (size_t)plan_cap));
     CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));

@@ -61,7 +61,9 @@ struct Engine {
     int dev = -1;
     int num_sms = 0;
     int smem_optin = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;   // compute
+    cudaStream_t copy_in = nullptr;  // host-to-device copies of the pipelined host calls
+    cudaStream_t copy_out = nullptr; // device-to-host copies
     std::recursive_mutex mu;
     Tuning tun;
     std::map<int64_t, PlanRec> plans;

@@ -532,11 +532,15 @@ int nbg_batch_create(const nbg_desc* descs, int64_t count, nbg_batch** out) {
         if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
             rc = fail(NBG_ECUDA, "stream create failed");
         } else {
+            constexpr int NSIDE = 4;
+            cudaStream_t side[NSIDE];
+            for (int i = 0; i < NSIDE; i++) cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking);
             if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
                 rc = fail(NBG_ECUDA, "begin capture failed");
             } else {
                 int64_t before = g_launches.load();
-                int rl = run_launches(E, bt->bb, bt->dmem, cs);
+                // a step's launches (one per shared-memory size) become parallel graph branches
+                int rl = run_launches_branched(E, bt->bb, bt->dmem, cs, side, NSIDE);
                 g_launches.store(before);  // captured, not issued
                 cudaError_t ec = cudaStreamEndCapture(cs, &bt->graph);
                 if (rl) rc = rl;
@@ -544,6 +548,7 @@ int nbg_batch_create(const nbg_desc* descs, int64_t count, nbg_batch** out) {
                 else if (cudaGraphInstantiate(&bt->exec, bt->graph, 0) != cudaSuccess)
                     rc = fail(NBG_ECUDA, "graph instantiate failed");
             }
+            for (int i = 0; i < NSIDE; i++) cudaStreamDestroy(side[i]);
             cudaStreamDestroy(cs);
         }
     }

@@ -830,6 +830,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
             });
         }
         Launch L{kind, (int64_t)bb.jobs.size(), (int64_t)v.size(), std::get<2>(kv.first)};
+        L.step = std::get<0>(kv.first);
         L.alg_ops = kv.second.ops;
         L.alg_bytes = kv.second.bytes;
         if ((int)L.smem > E.smem_optin) return fail(NBG_EINVAL, "tile needs %zu bytes of shared memory", L.smem);
@@ -880,6 +881,49 @@ int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st) 
         if (e != cudaSuccess) return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n,
                                           cudaGetErrorString(e));
         g_launches++;
+    }
+    return NBG_OK;
+}
+
+int run_launches_branched(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, cudaStream_t* side,
+                          int nside) {
+    const DProd* prods = (const DProd*)(dbase + bb.off_prods);
+    const Job* jobs = (const Job*)(dbase + bb.off_jobs);
+    size_t i = 0;
+    while (i < bb.launches.size()) {
+        size_t j = i;
+        while (j < bb.launches.size() && bb.launches[j].step == bb.launches[i].step) j++;
+        // launches [i, j) share a step: the first on st, the rest forked
+        std::vector<cudaEvent_t> joins;
+        cudaEvent_t fork = nullptr;
+        if (j - i > 1) {
+            CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+            CUDA_TRY(cudaEventRecord(fork, st));
+        }
+        for (size_t k = i; k < j; k++) {
+            const Launch& L = bb.launches[k];
+            cudaStream_t s = st;
+            if (k > i && nside > 0) {
+                s = side[(k - i - 1) % (size_t)nside];
+                CUDA_TRY(cudaStreamWaitEvent(s, fork, 0));
+            }
+            cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, jobs + L.off, L.n, L.smem, 0, s);
+            if (e != cudaSuccess)
+                return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n, cudaGetErrorString(e));
+            g_launches++;
+            if (s != st) {
+                cudaEvent_t jv;
+                CUDA_TRY(cudaEventCreateWithFlags(&jv, cudaEventDisableTiming));
+                CUDA_TRY(cudaEventRecord(jv, s));
+                joins.push_back(jv);
+            }
+        }
+        for (cudaEvent_t jv : joins) {
+            CUDA_TRY(cudaStreamWaitEvent(st, jv, 0));
+            cudaEventDestroy(jv);
+        }
+        if (fork) cudaEventDestroy(fork);
+        i = j;
     }
     return NBG_OK;
 }

@@ -98,6 +98,7 @@ struct Launch {
     int kind;
     int64_t off, n;
     size_t smem;
+    int step = 0;          // pipeline step: launches of one step are independent
     double alg_ops = 0;    // FP64 instructions of the reference schedule done by this launch
     double alg_bytes = 0;  // compulsory global bytes (operand/limb reads, tile loads and stores)
 };
@@ -115,5 +116,9 @@ struct BatchBuild {
 int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb);
 int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st);
 int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st);
+// Same, with the independent launches of each step forked onto `side`
+// streams (used while capturing a CUDA graph, where they become parallel branches).
+int run_launches_branched(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, cudaStream_t* side,
+                          int nside);
 
 }  // namespace nbg

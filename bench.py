@@ -237,13 +237,16 @@ def fp64_peak() -> dict:
     return {"dfma_per_s": fma.value, "dadd_per_s": add.value}
 
 
-def traffic_from_profiles(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+def traffic_from_profiles(kernel: str, point_primes: float):
+    """DRAM bytes of `kernel` for one batch: the committed ncu measurement of
+    bytes per transform point per prime (profiles/ncu_traffic.json, taken on
+    the 105*2^11-point class) times this batch's points x primes."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
-        return d.get(kernel, {}).get("bytes_per_launch_full_batch")
+        bpp = d.get("kernels", {}).get(kernel)
+        return None if bpp is None else float(bpp) * point_primes
     except (OSError, ValueError):
         return None
 
@@ -266,10 +269,12 @@ def run_ours(args, rank: int, world: int) -> None:
     d_out = torch.zeros(W["out_total"], dtype=torch.uint64, device=f"cuda:{dev}")
     ib, ob = d_in.data_ptr(), d_out.data_ptr()
     items = []
+    point_primes = 0.0  # sum over products of transform length x 2 primes
     for k in range(count):
         m, n, sq = int(W["m"][k]), int(W["n"][k]), bool(W["sq"][k])
         ba = bits_of(limbs, int(W["off_a"][k]), m)
         bb = ba if sq else bits_of(limbs, int(W["off_b"][k]), n)
+        point_primes += 2.0 * nbgpu.ntt_params(ba, bb)[1]
         items.append((ob + 8 * int(W["out_off"][k]), ib + 8 * int(W["off_a"][k]),
                       None if sq else ib + 8 * int(W["off_b"][k]), m, n, ba, bb))
     descs = nbgpu.make_descs(items)
@@ -345,10 +350,12 @@ def run_ours(args, rank: int, world: int) -> None:
         tot_ops = sum(st_["alg_ops"] for st_ in stats)
         roof = {
             "bound": "fp64", "kernel": dom, "achieved": achieved, "peak": pk, "unit": "T FP64 instr/s",
-            "frac": achieved / pk, "traffic": traffic_from_profiles(dom),
+            "frac": achieved / pk, "traffic": traffic_from_profiles(dom, point_primes),
+            "per": "one batch: all launches of the kernel in one step (launches are grouped by shared-memory size)",
             "peak_source": "measured: DFMA issue rate of libnbgpu_peak.so in this run (MEASURED_PEAKS.json has no FP64 figure)",
-            "alg_ops_per_launch": D["ops"] / D["launches"], "ms_per_launch": D["ms"] / D["launches"],
-            "hbm": {"alg_bytes_per_launch": D["bytes"] / D["launches"],
+            "alg_ops": D["ops"], "ms": D["ms"], "launches": D["launches"],
+            "traffic_source": "profiles/ncu_traffic.json bytes per point per prime x this batch's points",
+            "hbm": {"alg_bytes": D["bytes"],
                     "achieved_gbs": D["bytes"] / (D["ms"] / 1e3) / 1e9, "peak_gbs": 6542.7,
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
             "kernels": {k: {"ms_per_step": v["ms"], "share": v["ms"] / sum(x["ms"] for x in kern.values()),

@@ -109,6 +109,48 @@ int nbg_batch_stats(const nbg_batch *bt, int32_t *kinds, int64_t *njobs, double 
  * CUDA event between launches; ms[i] = duration of launch i. */
 int nbg_batch_profile(nbg_batch *bt, void *stream, float *ms, int32_t cap);
 
+/* ---- serving: continuous batching ------------------------------------------ */
+
+/* A server owns a worker thread and an HBM arena of hbm_budget_bytes.
+ * Requests submitted from any thread are batched as they arrive: while earlier
+ * batches run (up to three in flight, each on its own stream) the worker forms
+ * the next one from everything pending that fits in the free arena.
+ * max_batch bounds a batch (0: no bound); max_queue bounds pending requests
+ * (0: no bound; past it nbg_submit returns NBG_EBUSY). */
+typedef struct nbg_server_opts {
+    int64_t hbm_budget_bytes;
+    int64_t max_batch;
+    int64_t max_queue;
+} nbg_server_opts;
+
+typedef struct nbg_server_stats_t {
+    int64_t completed;
+    int64_t failed;
+    int64_t pending;
+    int32_t in_flight_batches;
+    int32_t reserved;
+    double p50_ms;             /* submit-to-completion latency percentiles */
+    double p99_ms;
+    double output_limbs_per_s; /* completed output limbs / (last completion - first submit) */
+} nbg_server_stats_t;
+
+typedef struct nbg_server nbg_server;
+int nbg_server_create(const nbg_server_opts *opts, nbg_server **out);
+/* Host request: operands read (and the result written) through host pointers;
+ * the buffers must stay valid until the request completes.  Returns a ticket. */
+int nbg_submit(nbg_server *s, const nbg_desc *d, int64_t *ticket);
+/* Device-resident request: device pointers, bits_a/bits_b required. */
+int nbg_submit_dev(nbg_server *s, const nbg_desc *d, int64_t *ticket);
+/* *done = 1 once the request finished; returns its status. */
+int nbg_poll(nbg_server *s, int64_t ticket, int32_t *done);
+/* Waits at most timeout_us for the request (NBG_ETIMEOUT after that). */
+int nbg_wait(nbg_server *s, int64_t ticket, int64_t timeout_us);
+/* Forgets a finished request's record. */
+int nbg_release(nbg_server *s, int64_t ticket);
+int nbg_server_stats(nbg_server *s, nbg_server_stats_t *st);
+/* Drains the queue, stops the worker, frees the arena. */
+int nbg_server_destroy(nbg_server *s);
+
 /* ---- admission (host-side restatement of the reference's sizing) -------- */
 
 /* fp_ntt_params (src/fpntt.jl:964-977): chunk width b and transform length N. */

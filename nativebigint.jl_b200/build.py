@@ -26,7 +26,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
              "-Wno-unused-parameter", f"-I{CUDA}/include"]
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu"]
-CXX_SOURCES = ["engine.cpp", "api.cpp"]
+CXX_SOURCES = ["engine.cpp", "api.cpp", "serve.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

@@ -36,6 +36,8 @@ EXPORTS = [
     "nbg_ntt_rev_dev", "nbg_pointwise_dev", "nbg_unpack_dev", "nbg_plan_info", "nbg_plan_layout", "nbg_set_tuning",
     "nbg_get_tuning", "nbg_init", "nbg_last_error", "nbg_default_stream", "nbg_launch_count",
     "nbg_mul_dev_noalloc", "nbg_load_tuning", "nbg_version", "nbg_trim_plans",
+    "nbg_server_create", "nbg_submit", "nbg_submit_dev", "nbg_poll", "nbg_wait", "nbg_release",
+    "nbg_server_stats", "nbg_server_destroy",
 ]
 
 
@@ -93,6 +95,14 @@ def lib() -> ctypes.CDLL:
             "nbg_set_tuning": [c.c_char_p],
             "nbg_get_tuning": [c.c_char_p, i64],
             "nbg_init": [i32],
+            "nbg_server_create": [vp, c.POINTER(vp)],
+            "nbg_submit": [vp, vp, c.POINTER(i64)],
+            "nbg_submit_dev": [vp, vp, c.POINTER(i64)],
+            "nbg_poll": [vp, i64, c.POINTER(i32)],
+            "nbg_wait": [vp, i64, i64],
+            "nbg_release": [vp, i64],
+            "nbg_server_stats": [vp, vp],
+            "nbg_server_destroy": [vp],
             "nbg_load_tuning": [c.c_char_p],
         }
         for name, args in sig.items():
@@ -268,6 +278,72 @@ class Batch:
     def close(self) -> None:
         if self._h:
             lib().nbg_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# serving (continuous batching)
+
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("max_batch", ctypes.c_int64), ("max_queue", ctypes.c_int64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("pending", ctypes.c_int64),
+                ("in_flight_batches", ctypes.c_int32), ("reserved", ctypes.c_int32), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("output_limbs_per_s", ctypes.c_double)]
+
+
+class Server:
+    """Continuous-batching product server (nbg_server_*)."""
+
+    def __init__(self, hbm_budget_bytes: int = 1 << 30, max_batch: int = 0, max_queue: int = 0):
+        self._h = ctypes.c_void_p()
+        opts = ServerOpts(hbm_budget_bytes, max_batch, max_queue)
+        _check(lib().nbg_server_create(ctypes.byref(opts), ctypes.byref(self._h)))
+        self._keep: dict = {}
+
+    def submit(self, a: np.ndarray, b, r: np.ndarray) -> int:
+        """Host request: r (len(a)+len(b) limbs) receives a*b (b None: a^2)."""
+        a = _u64(a)
+        d = NbgDesc(_ptr(r), _ptr(a), None if b is None else _ptr(b), a.size, a.size if b is None else b.size, 0, 0)
+        t = ctypes.c_int64()
+        _check(lib().nbg_submit(self._h, ctypes.byref(d), ctypes.byref(t)))
+        self._keep[t.value] = (a, b, r)
+        return t.value
+
+    def submit_dev(self, r, a, m: int, b, n: int, bits_a: int, bits_b: int) -> int:
+        d = NbgDesc(_dptr(r), _dptr(a), None if b is None else _dptr(b), m, n, bits_a, bits_b)
+        t = ctypes.c_int64()
+        _check(lib().nbg_submit_dev(self._h, ctypes.byref(d), ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        done = ctypes.c_int32()
+        _check(lib().nbg_poll(self._h, ticket, ctypes.byref(done)))
+        return bool(done.value)
+
+    def wait(self, ticket: int, timeout_s: float = 60.0) -> None:
+        _check(lib().nbg_wait(self._h, ticket, int(timeout_s * 1e6)))
+        self._keep.pop(ticket, None)
+
+    def release(self, ticket: int) -> None:
+        _check(lib().nbg_release(self._h, ticket))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().nbg_server_stats(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_ if k != "reserved"}
+
+    def close(self) -> None:
+        if self._h:
+            lib().nbg_server_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

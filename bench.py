@@ -444,6 +444,166 @@ def run_ours(args, rank: int, world: int) -> None:
     bt.close()
 
 
+SERVE_WORKLOAD = ("Poisson arrivals of products: larger operand log-uniform [152, 2^20] limbs, ratio U[0.25,1], "
+                  "uniform random limbs, device-resident operands and results, 60 GB HBM admission budget")
+
+
+def run_serve(args) -> None:
+    """Serving loop at swept Poisson arrival rates, one JSON line per rate.
+
+    A pool of `serve_pool` products (sizes as SERVE_WORKLOAD) stays resident on
+    the device.  Each generation of requests is a fresh random permutation of
+    the pool, so each generation writes every pool slot once; the results go to
+    one of RING copies of the pool's output area, and before a copy is reused
+    every request that wrote it is waited for and the whole copy is compared
+    with the GMP products on the device (every result is checked).  Latency is
+    the server's submit-to-completion time; `submit_lag` is how far the Python
+    submission loop fell behind the Poisson schedule."""
+    import torch
+
+    import nbgpu
+    import oracle
+
+    RING = 4
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    L = nbgpu.lib()
+    nbgpu._check(L.nbg_init(dev))
+    rng = np.random.Generator(np.random.PCG64(args.seed))
+    P = args.serve_pool
+    m = np.exp(rng.uniform(math.log(152), math.log(1 << 20), P)).astype(np.int64)
+    n = np.maximum(1, np.round(m * rng.uniform(0.25, 1.0, P)).astype(np.int64))
+    ops = []
+    for k in range(P):
+        a = rng.integers(0, 2**64, int(m[k]), dtype=np.uint64)
+        b = rng.integers(0, 2**64, int(n[k]), dtype=np.uint64)
+        a[-1] = a[-1] or np.uint64(1)
+        b[-1] = b[-1] or np.uint64(1)
+        ops.append((a, b))
+    out_off = np.concatenate([[0], np.cumsum(m + n)[:-1]]).astype(np.int64)
+    out_total = int((m + n).sum())
+    # GMP products of the pool (threads: ctypes releases the GIL)
+    gold_h = np.zeros(out_total, dtype=np.uint64)
+
+    def gmp_one(k):
+        gold_h[out_off[k]: out_off[k] + m[k] + n[k]] = oracle.gmp_mul(*ops[k])
+
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        list(ex.map(gmp_one, sorted(range(P), key=lambda k: -int(m[k] + n[k]))))
+    gold = torch.from_numpy(gold_h).cuda()
+    d_ops = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in ops]
+    ring = [torch.zeros(out_total, dtype=torch.uint64, device="cuda") for _ in range(RING)]
+    # per-slot boundaries for the per-product mismatch count
+    bounds = torch.from_numpy(np.concatenate([out_off, [out_total]])).cuda()
+    descs = []
+    for c in range(RING):
+        row = (nbgpu.NbgDesc * P)()
+        for k in range(P):
+            da, db = d_ops[k]
+            row[k] = nbgpu.NbgDesc(ring[c].data_ptr() + 8 * int(out_off[k]), da.data_ptr(), db.data_ptr(),
+                                   int(m[k]), int(n[k]), oracle.magnitude_bits(ops[k][0]),
+                                   oracle.magnitude_bits(ops[k][1]))
+        descs.append(row)
+    torch.cuda.synchronize()
+    # capacity reference: the whole pool as one batch (graph replay), same products
+    bt = nbgpu.Batch(descs[0])
+    s0 = torch.cuda.current_stream()
+    for _ in range(2):
+        bt.run(s0.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s0)
+    for _ in range(5):
+        bt.run(s0.cuda_stream)
+    e1.record(s0)
+    torch.cuda.synchronize()
+    pool_batch_rate = out_total * 5 / (e0.elapsed_time(e1) / 1e3)
+    bt.close()
+
+    def check_copy(c: int, slots) -> int:
+        """Products among `slots` in ring copy c that differ from GMP."""
+        bad = (ring[c] != gold).to(torch.int64).cumsum(0)
+        bad = torch.cat([torch.zeros(1, dtype=torch.int64, device="cuda"), bad])
+        per = bad[bounds[1:]] - bad[bounds[:-1]]
+        idx = torch.as_tensor(np.asarray(slots, dtype=np.int64), device="cuda")
+        return int((per[idx] != 0).sum().item())
+
+    rates = [float(x) for x in args.serve_rates.split(",") if x]
+    for rate in rates:
+        srv = nbgpu.Server(hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)))
+        h = srv._h
+        ticket = ctypes.c_int64()
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, int(rate * args.serve_seconds * 1.05) + 16))
+        arrivals = arrivals[arrivals < args.serve_seconds]
+        gen_tickets: list[list[int]] = []
+        gen_slots: list[list[int]] = []
+        mismatches, stalls, stall_s = 0, 0, 0.0
+        lags = np.zeros(len(arrivals))
+        submitted_limbs = 0
+        perm = None
+        for c in range(RING):
+            ring[c].zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i, ta in enumerate(arrivals):
+            g, j = divmod(i, P)
+            if j == 0:
+                perm = rng.permutation(P)
+                if g >= RING:  # reuse ring copy g % RING: its generation must be done, then checked
+                    ts = time.perf_counter()
+                    waited = False
+                    for t in gen_tickets[g - RING]:
+                        if not waited:
+                            done = ctypes.c_int32()
+                            L.nbg_poll(h, t, ctypes.byref(done))
+                            waited = not done.value
+                        nbgpu._check(L.nbg_wait(h, t, 600_000_000))
+                        L.nbg_release(h, t)
+                    stalls += int(waited)
+                    stall_s += time.perf_counter() - ts
+                    mismatches += check_copy(g % RING, gen_slots[g - RING])
+                    ring[g % RING].zero_()
+                    torch.cuda.current_stream().synchronize()
+                gen_tickets.append([])
+                gen_slots.append([])
+            k = int(perm[j])
+            gen_slots[g].append(k)
+            while time.perf_counter() - t0 < ta:
+                pass
+            lags[i] = time.perf_counter() - t0 - ta
+            nbgpu._check(L.nbg_submit_dev(h, ctypes.byref(descs[g % RING], k * ctypes.sizeof(nbgpu.NbgDesc)),
+                                          ctypes.byref(ticket)))
+            gen_tickets[g].append(ticket.value)
+            submitted_limbs += int(m[k] + n[k])
+        t_sub = time.perf_counter() - t0
+        for g in range(max(0, len(gen_tickets) - RING), len(gen_tickets)):
+            for t in gen_tickets[g]:
+                nbgpu._check(L.nbg_wait(h, t, 600_000_000))
+            mismatches += check_copy(g % RING, gen_slots[g])
+        t_all = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        count = len(arrivals)
+        line = {
+            "metric": "serving: sustained output limbs/s and submit-to-completion latency", "impl": "ours",
+            "mode": "serve", "unit": "output limbs/s", "value": st["output_limbs_per_s"],
+            "offered_rate": rate, "submitted_rate": count / t_sub if t_sub > 0 else None,
+            "requests": count, "completed": st["completed"], "failed": st["failed"],
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "submit_lag_p99_ms": float(np.percentile(lags, 99) * 1e3) if count else None,
+            "wall_s": t_all, "output_limbs": submitted_limbs,
+            "ring_stalls": stalls, "ring_stall_s": stall_s,
+            "batches": st["batches"], "mean_batch_requests": st["mean_batch_requests"],
+            "pool_as_one_batch": {"value": pool_batch_rate, "unit": "output limbs/s"},
+            "bitexact": {"checked_vs_gmp": count, "mismatches": mismatches},
+            "dtype": "f64", "data": "synthetic", "n_gpus": 1,
+            "config": {"workload": SERVE_WORKLOAD, "pool_products": P, "pool_output_limbs": out_total,
+                       "hbm_budget_gb": args.serve_budget_gb, "seconds": args.serve_seconds, "seed": args.seed},
+        }
+        print(json.dumps(line), flush=True)
+        if mismatches or st["failed"]:
+            raise SystemExit(f"serve: {mismatches} mismatches, {st['failed']} failed at rate {rate}")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -457,6 +617,11 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--shape", default="", help="m,n: a batch of one product shape instead of the mixed workload")
     ap.add_argument("--square", action="store_true", help="with --shape: squares of m-limb operands")
+    ap.add_argument("--serve", action="store_true", help="serving loop at swept Poisson arrival rates")
+    ap.add_argument("--serve-rates", default="1000,5000,20000,50000,200000")
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-pool", type=int, default=600)
+    ap.add_argument("--serve-budget-gb", type=float, default=60.0)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -469,7 +634,10 @@ def main() -> None:
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        if args.impl == "reference":
+        if args.serve:
+            if rank == 0:
+                run_serve(args)
+        elif args.impl == "reference":
             run_reference(args, rank, world)
         else:
             run_ours(args, rank, world)

@@ -115,12 +115,17 @@ int nbg_batch_profile(nbg_batch *bt, void *stream, float *ms, int32_t cap);
  * Requests submitted from any thread are batched as they arrive: while earlier
  * batches run (up to three in flight, each on its own stream) the worker forms
  * the next one from everything pending that fits in the free arena.
- * max_batch bounds a batch (0: no bound); max_queue bounds pending requests
- * (0: no bound; past it nbg_submit returns NBG_EBUSY). */
+ * A new batch starts at once while fewer than two batches are in flight;
+ * with two or more it starts when the pending requests hold at least
+ * batch_points transform points (0: 2^23), so that under load batches stay
+ * large enough to fill the GPU while an idle GPU still takes a lone request
+ * immediately.  max_batch bounds a batch (0: no bound); max_queue bounds
+ * pending requests (0: no bound; past it nbg_submit returns NBG_EBUSY). */
 typedef struct nbg_server_opts {
     int64_t hbm_budget_bytes;
     int64_t max_batch;
     int64_t max_queue;
+    int64_t batch_points;
 } nbg_server_opts;
 
 typedef struct nbg_server_stats_t {
@@ -132,6 +137,8 @@ typedef struct nbg_server_stats_t {
     double p50_ms;             /* submit-to-completion latency percentiles */
     double p99_ms;
     double output_limbs_per_s; /* completed output limbs / (last completion - first submit) */
+    int64_t batches;           /* batches launched */
+    double mean_batch_requests;
 } nbg_server_stats_t;
 
 typedef struct nbg_server nbg_server;

@@ -757,78 +757,97 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
     };
     // key: (step order, kind, smem)
     std::map<std::tuple<int, int, size_t>, Group> groups;
-    auto add_job = [&](int order, int kind, size_t smem, const Job& j, double ops, double bytes) {
-        Group& g = groups[std::make_tuple(order, kind, smem)];
-        g.jobs.push_back(j);
-        g.ops += ops;
-        g.bytes += bytes;
+    auto group_of = [&](int order, int kind, size_t smem) -> Group& {
+        return groups[std::make_tuple(order, kind, smem)];
     };
     // step order: forward steps 0..pmax-2, the pointwise step pmax-1, reverse
     // steps pmax..2pmax-2, unpack 2pmax-1, carry 2pmax
-    for (int64_t k = 0; k < count; k++) {
-        const DProd& P = bb.prods[(size_t)k];
-        const DPlan& pl = bb.plan_of[(size_t)k]->d;
-        const int Pn = P.npass;
-        const double nops = P.sqr ? 1.0 : 2.0;
+    //
+    // Products of one plan share every pass shape, so transform jobs are
+    // emitted per plan class, with no per-job sorting: classes by transform
+    // length (longest first, so the tail of each launch is short), then tile,
+    // then operand, then product.  CTAs that run together read the same
+    // twiddle slice, which comes from DRAM once and from L2 for the rest.
+    std::vector<int32_t> byclass((size_t)count);
+    for (int64_t k = 0; k < count; k++) byclass[(size_t)k] = (int32_t)k;
+    std::stable_sort(byclass.begin(), byclass.end(), [&](int32_t x, int32_t y) {
+        const int64_t nx = bb.plan_of[(size_t)x]->d.N, ny = bb.plan_of[(size_t)y]->d.N;
+        if (nx != ny) return nx > ny;
+        return bb.prods[(size_t)x].plan < bb.prods[(size_t)y].plan;
+    });
+    std::vector<int32_t> cls;
+    for (size_t i = 0; i < byclass.size();) {
+        const int slot = bb.prods[(size_t)byclass[i]].plan;
+        cls.clear();
+        double sum_bch = 0;
+        while (i < byclass.size() && bb.prods[(size_t)byclass[i]].plan == slot) {
+            sum_bch += bb.prods[(size_t)byclass[i]].bch;
+            cls.push_back(byclass[i++]);
+        }
+        const DProd& P0 = bb.prods[(size_t)cls[0]];
+        const DPlan& pl = bb.plan_of[(size_t)cls[0]]->d;
+        const int Pn = P0.npass;
+        const int nop = P0.sqr ? 1 : 2;
+        const double nc = (double)cls.size();
+        auto emit = [&](Group& g, const DPass& ps, int nopnd, int sub_base) {
+            for (int64_t t = 0; t < ps.ntiles; t++)
+                for (int op = 0; op < nopnd; op++)
+                    for (int32_t k : cls) g.jobs.push_back(Job{k, sub_base | (op << 1), t});
+        };
         for (int p = 0; p < Pn - 1; p++) {
             const DPass& ps = pl.pass[p];
             const size_t smem = sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
-            const double ops = 2.0 * pass_ops(pl, ps, true);
-            for (int op = 0; op < (P.sqr ? 1 : 2); op++) {
-                const double in_b = p == 0 ? pts * P.bch / 8.0 : 2.0 * 8.0 * pts;
-                for (int64_t t = 0; t < ps.ntiles; t++)
-                    add_job(pmax - Pn + p, JK_FWD, smem, Job{(int32_t)k, (op << 1) | (p << 8), t}, ops,
-                            in_b + 2.0 * 8.0 * pts);
-            }
+            const double jobs = (double)ps.ntiles * nop * nc;
+            Group& g = group_of(pmax - Pn + p, JK_FWD, smem);
+            emit(g, ps, nop, p << 8);
+            g.ops += jobs * 2.0 * pass_ops(pl, ps, true);
+            // first pass reads packed limbs (bch bits per point), later ones both primes' doubles
+            const double in_b = p == 0 ? (double)ps.ntiles * nop * pts * sum_bch / 8.0 : jobs * 2.0 * 8.0 * pts;
+            g.bytes += in_b + jobs * 2.0 * 8.0 * pts;
         }
         {
             const DPass& ps = pl.pass[Pn - 1];
-            const size_t smem = sizeof(double) * (P.sqr ? 2 : 4) * (size_t)tile_stride_doubles(ps.G * ps.C);
+            const size_t smem = sizeof(double) * (P0.sqr ? 2 : 4) * (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
-            const double ops = 2.0 * (nops * pass_ops(pl, ps, true) + 7.0 * pts + pass_ops(pl, ps, false));
-            const double in_b = Pn == 1 ? nops * pts * P.bch / 8.0 : 2.0 * nops * 8.0 * pts;
-            for (int64_t t = 0; t < ps.ntiles; t++)
-                add_job(pmax - 1, JK_PWR, smem, Job{(int32_t)k, (Pn - 1) << 8, t}, ops, in_b + 2.0 * 8.0 * pts);
+            const double jobs = (double)ps.ntiles * nc;
+            Group& g = group_of(pmax - 1, JK_PWR, smem);
+            emit(g, ps, 1, (Pn - 1) << 8);
+            g.ops += jobs * 2.0 * (nop * pass_ops(pl, ps, true) + 7.0 * pts + pass_ops(pl, ps, false));
+            const double in_b = Pn == 1 ? (double)ps.ntiles * nop * pts * sum_bch / 8.0 : jobs * 2.0 * nop * 8.0 * pts;
+            g.bytes += in_b + jobs * 2.0 * 8.0 * pts;
         }
         for (int p = Pn - 2; p >= 0; p--) {
             const DPass& ps = pl.pass[p];
             const size_t smem = sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
-            for (int64_t t = 0; t < ps.ntiles; t++)
-                add_job(pmax + (Pn - 2 - p), JK_REV, smem, Job{(int32_t)k, p << 8, t}, 2.0 * pass_ops(pl, ps, false),
-                        2.0 * 16.0 * pts);
+            const double jobs = (double)ps.ntiles * nc;
+            Group& g = group_of(pmax + (Pn - 2 - p), JK_REV, smem);
+            emit(g, ps, 1, p << 8);
+            g.ops += jobs * 2.0 * pass_ops(pl, ps, false);
+            g.bytes += jobs * 2.0 * 16.0 * pts;
         }
     }
     const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / bmin + 4;
     const size_t unp_smem = sizeof(uint64_t) * 2 * (size_t)align_up((size_t)ncoef, 2);
+    Group& gu = group_of(2 * pmax - 1, JK_UNPACK, unp_smem);
     for (int64_t k = 0; k < count; k++) {
         const DProd& P = bb.prods[(size_t)k];
-        const double per_tile_ops = 28.0 * (double)P.nconv / (double)P.ntl;
-        const double per_tile_bytes = (16.0 * (double)P.nconv + 8.0 * (double)P.rn) / (double)P.ntl;
-        for (int64_t t = 0; t < P.ntl; t++)
-            add_job(2 * pmax - 1, JK_UNPACK, unp_smem, Job{(int32_t)k, 0, t}, per_tile_ops, per_tile_bytes);
-        if (P.ntl > 1) add_job(2 * pmax, JK_CARRY, 0, Job{(int32_t)k, 0, 0}, 0.0, 4.0 * (double)P.ntl);
+        for (int64_t t = 0; t < P.ntl; t++) gu.jobs.push_back(Job{(int32_t)k, 0, t});
+        gu.ops += 28.0 * (double)P.nconv;
+        gu.bytes += 16.0 * (double)P.nconv + 8.0 * (double)P.rn;
+        if (P.ntl > 1) {
+            Group& gc = group_of(2 * pmax, JK_CARRY, 0);
+            gc.jobs.push_back(Job{(int32_t)k, 0, 0});
+            gc.bytes += 4.0 * (double)P.ntl;
+        }
     }
-    // Within a launch: jobs ordered so CTAs that run together share twiddle
-    // columns — by plan (transform length), then tile, then product.  Every
-    // product of one length reads the same twiddle slice for the same tile, so
-    // the slice comes from DRAM once and from L2 for the rest.  Biggest plans
-    // first so the tail of each launch is short.
+    size_t total_jobs = 0;
+    for (auto& kv : groups) total_jobs += kv.second.jobs.size();
+    bb.jobs.reserve(total_jobs);
     for (auto& kv : groups) {
         const int kind = std::get<1>(kv.first);
         std::vector<Job>& v = kv.second.jobs;
-        if (kind == JK_FWD || kind == JK_REV || kind == JK_PWR) {
-            std::stable_sort(v.begin(), v.end(), [&](const Job& x, const Job& y) {
-                const DPlan& px = bb.plan_of[(size_t)x.prod]->d;
-                const DPlan& py = bb.plan_of[(size_t)y.prod]->d;
-                if (px.N != py.N) return px.N > py.N;
-                const int sx = bb.prods[(size_t)x.prod].plan, sy = bb.prods[(size_t)y.prod].plan;
-                if (sx != sy) return sx < sy;
-                if (x.tile != y.tile) return x.tile < y.tile;
-                return x.sub < y.sub;
-            });
-        }
         Launch L{kind, (int64_t)bb.jobs.size(), (int64_t)v.size(), std::get<2>(kv.first)};
         L.step = std::get<0>(kv.first);
         L.alg_ops = kv.second.ops;
@@ -836,6 +855,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         if ((int)L.smem > E.smem_optin) return fail(NBG_EINVAL, "tile needs %zu bytes of shared memory", L.smem);
         bb.launches.push_back(L);
         bb.jobs.insert(bb.jobs.end(), v.begin(), v.end());
+        std::vector<Job>().swap(v);
     }
 
     // device layout: [prods | jobs | work | agg]
@@ -847,8 +867,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
     return NBG_OK;
 }
 
-// Point the descriptors at the device block and upload descriptors + jobs.
-int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st) {
+void bind_batch(BatchBuild& bb, char* dbase) {
     double* work = (double*)(dbase + bb.off_work);
     uint32_t* agg = (uint32_t*)(dbase + bb.off_agg);
     for (size_t k = 0; k < bb.prods.size(); k++) {
@@ -864,6 +883,17 @@ int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st) {
         }
         P.agg = agg + bb.agg_off[k];
     }
+}
+
+void stage_batch(const BatchBuild& bb, char* host) {
+    memset(host, 0, bb.off_work);
+    memcpy(host + bb.off_prods, bb.prods.data(), sizeof(DProd) * bb.prods.size());
+    if (!bb.jobs.empty()) memcpy(host + bb.off_jobs, bb.jobs.data(), sizeof(Job) * bb.jobs.size());
+}
+
+// Point the descriptors at the device block and upload descriptors + jobs.
+int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st) {
+    bind_batch(bb, dbase);
     CUDA_TRY(cudaMemcpyAsync(dbase + bb.off_prods, bb.prods.data(), sizeof(DProd) * bb.prods.size(),
                              cudaMemcpyHostToDevice, st));
     if (!bb.jobs.empty())

@@ -115,6 +115,12 @@ struct BatchBuild {
 
 int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb);
 int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st);
+// Points each product's workspace and carry words into the batch's device
+// region at dbase (what upload_batch does before copying).
+void bind_batch(BatchBuild& bb, char* dbase);
+// Writes the bound descriptors and job list into `host` in their device
+// layout: off_work bytes that one copy to dbase makes the region's head.
+void stage_batch(const BatchBuild& bb, char* host);
 int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st);
 // Same, with the independent launches of each step forked onto `side`
 // streams (used while capturing a CUDA graph, where they become parallel branches).

@@ -38,6 +38,8 @@ using namespace nbg;
 namespace {
 
 constexpr int MAX_FLIGHT = 3;
+constexpr int NSIDE = 3;                     // side streams per slot: a step's launches run side by side
+constexpr int64_t DEFAULT_BATCH_POINTS = int64_t(1) << 23;
 
 double now_us() {
     return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -92,6 +94,7 @@ class Arena {
 struct Request {
     ProdIn in;
     bool host = false;
+    double points = 0;  // transform length (what the request costs the GPU, roughly)
     double t_submit = 0, t_done = 0;
     int state = 0;  // 0 pending, 1 in flight, 2 done, 3 failed
     int rc = 0;
@@ -104,9 +107,14 @@ struct Flight {
     int slot = -1;
     cudaEvent_t done = nullptr;
     cudaStream_t st = nullptr;
-    // host requests: operands and results staged in the slot's pinned buffer
-    char* hstage = nullptr;
-    std::vector<std::pair<size_t, int64_t>> host_results;  // staging offset, request id
+    // host requests: results staged in the slot's pinned buffer, copied to
+    // the caller's buffer on retirement
+    struct HostResult {
+        size_t stage_off;
+        uint64_t* dst;
+        size_t bytes;
+    };
+    std::vector<HostResult> host_results;
 };
 
 }  // namespace
@@ -125,179 +133,219 @@ struct nbg_server {
     std::deque<Flight> flights;
     // one stream and one pinned staging buffer per flight slot
     cudaStream_t streams[MAX_FLIGHT] = {};
+    cudaStream_t side[MAX_FLIGHT][NSIDE] = {};
     char* pinned[MAX_FLIGHT] = {};
     size_t pinned_bytes[MAX_FLIGHT] = {};
     bool slot_busy[MAX_FLIGHT] = {};
     std::vector<double> latencies_us;
-    int64_t completed = 0, failed = 0;
+    int64_t completed = 0, failed = 0, batches = 0, batched_requests = 0;
+    double pending_points = 0;
+    bool wake = false;  // a submission or a batch completion since the worker last looked
     double limbs_done = 0, t_first = 0, t_last = 0;
 
     void run();
     bool launch_batch(std::unique_lock<std::mutex>& lk);
-    void retire(std::unique_lock<std::mutex>& lk, bool wait_one);
+    void retire(std::unique_lock<std::mutex>& lk);
+    void fail_front(int rc);
+    static void CUDART_CB on_batch_done(void* self);
 };
 
-// Forms one batch from the front of the queue, within the arena.  Called with
-// the server lock held; the engine lock is taken inside.
+// Fails the request at the front of the queue (server lock held).
+void nbg_server::fail_front(int rc) {
+    Request& q = reqs[pending.front()];
+    pending_points -= q.points;
+    q.state = 3;
+    q.rc = rc;
+    q.t_done = now_us();
+    failed++;
+    pending.pop_front();
+    cv_done.notify_all();
+}
+
+// Forms one batch from the front of the queue, within the free arena, and
+// launches it.  Entered and left with the server lock held, but the lock is
+// dropped while the batch is built, staged and launched so that submitters
+// never wait for that host work.  Only the worker thread pops the queue and
+// touches the arena, the slots and the flight list's contents, so the
+// requests at the front stay where they are meanwhile.
 bool nbg_server::launch_batch(std::unique_lock<std::mutex>& lk) {
     if (pending.empty() || (int)flights.size() >= MAX_FLIGHT) return false;
+    const double target = (double)(opts.batch_points > 0 ? opts.batch_points : DEFAULT_BATCH_POINTS);
+    if (flights.size() >= 2 && pending_points < target) return false;  // let the next batch grow
     std::vector<int64_t> ids;
     std::vector<ProdIn> in;
-    size_t host_in = 0, host_out = 0;
+    std::vector<char> host;
     const int64_t maxb = opts.max_batch > 0 ? opts.max_batch : 100000;
     for (int64_t id : pending) {
         if ((int64_t)ids.size() >= maxb) break;
         const Request& q = reqs[id];
         ids.push_back(id);
         in.push_back(q.in);
-        if (q.host) {  // each operand padded on its own, as laid out below
-            host_in += up256(8 * (size_t)q.in.m) + (q.in.sqr ? 0 : up256(8 * (size_t)q.in.n));
-            host_out += up256(8 * (size_t)(q.in.m + q.in.n));
-        }
+        host.push_back(q.host);
     }
+    lk.unlock();
     Engine& E = g_eng;
-    std::lock_guard<std::recursive_mutex> elk(E.mu);
-    // shrink the batch until it fits in the free arena
     Flight f;
-    size_t off = 0;
-    for (;;) {
-        int rc = build_batch(E, in.data(), (int64_t)in.size(), f.bb);
-        if (rc) {  // a request the engine refuses (size): fail it alone
+    size_t off = 0, host_in = 0, host_out = 0;
+    int refuse = 0;
+    {
+        std::lock_guard<std::recursive_mutex> elk(E.mu);
+        // shrink the batch until it fits in the free arena
+        for (;;) {
+            int rc = build_batch(E, in.data(), (int64_t)in.size(), f.bb);
+            if (rc) {  // a request the engine refuses (size): fail it alone
+                if (in.size() == 1) {
+                    refuse = rc;
+                    break;
+                }
+                in.resize(in.size() / 2);
+                continue;
+            }
+            host_in = host_out = 0;
+            for (size_t k = 0; k < in.size(); k++)
+                if (host[k]) {  // each operand padded on its own, as laid out below
+                    host_in += up256(8 * (size_t)in[k].m) + (in[k].sqr ? 0 : up256(8 * (size_t)in[k].n));
+                    host_out += up256(8 * (size_t)(in[k].m + in[k].n));
+                }
+            f.bytes = up256(f.bb.dev_bytes) + host_in + host_out;
+            if (arena.alloc(f.bytes, off)) break;
             if (in.size() == 1) {
-                Request& q = reqs[ids[0]];
-                q.state = 3;
-                q.rc = rc;
-                q.t_done = now_us();
-                failed++;
-                pending.pop_front();
-                cv_done.notify_all();
-                return true;
+                if (f.bytes > arena.size())  // can never fit
+                    refuse = fail(NBG_ENOMEM, "request needs %zu bytes, over the server's HBM budget", f.bytes);
+                else
+                    refuse = -1;  // wait for memory to free up
+                break;
             }
             in.resize(in.size() / 2);
-            ids.resize(in.size());
-            continue;
         }
-        host_in = host_out = 0;
-        for (int64_t id : ids)
-            if (reqs[id].host) {
-                const ProdIn& q = reqs[id].in;
-                host_in += up256(8 * (size_t)q.m) + (q.sqr ? 0 : up256(8 * (size_t)q.n));
-                host_out += up256(8 * (size_t)(q.m + q.n));
-            }
-        f.bytes = up256(f.bb.dev_bytes) + host_in + host_out;
-        if (arena.alloc(f.bytes, off)) break;
-        if (f.bytes > arena.size() && in.size() == 1) {  // can never fit
-            Request& q = reqs[ids[0]];
-            q.state = 3;
-            q.rc = fail(NBG_ENOMEM, "request needs %zu bytes, over the server's HBM budget", f.bytes);
-            q.t_done = now_us();
-            failed++;
-            pending.pop_front();
-            cv_done.notify_all();
-            return true;
-        }
-        if (in.size() == 1) return false;  // wait for memory to free up
-        in.resize(in.size() / 2);
-        ids.resize(in.size());
     }
+    if (refuse) {
+        lk.lock();
+        if (refuse < 0) return false;
+        fail_front(refuse);
+        return true;
+    }
+    ids.resize(in.size());
     f.off = off;
     char* base = dmem + off;
     int slot = 0;
     while (slot_busy[slot]) slot++;  // flights.size() < MAX_FLIGHT: a slot is free
     f.slot = slot;
     f.st = streams[slot];
-    // host requests: gather operands into the slot's pinned staging, one copy in
+    // The slot's pinned buffer holds [descriptors and jobs | host operands |
+    // host results]; descriptors and operands go over in one copy each.
+    const size_t head = f.bb.off_work;
     const size_t dev_in = up256(f.bb.dev_bytes), dev_out = dev_in + host_in;
-    if (host_in) {
-        if (pinned_bytes[slot] < host_in + host_out) {
-            if (pinned[slot]) cudaFreeHost(pinned[slot]);
-            pinned[slot] = nullptr;
-            pinned_bytes[slot] = 0;
-            const size_t want = std::max(host_in + host_out, (size_t)(8 << 20));
-            if (cudaMallocHost(&pinned[slot], want) != cudaSuccess) {
-                cudaGetLastError();
-                arena.release(off, f.bytes);
-                return false;
-            }
-            pinned_bytes[slot] = want;
+    const size_t need = up256(head) + host_in + host_out;
+    if (pinned_bytes[slot] < need) {
+        if (pinned[slot]) cudaFreeHost(pinned[slot]);
+        pinned[slot] = nullptr;
+        pinned_bytes[slot] = 0;
+        const size_t want = std::max(need + need / 4, (size_t)(8 << 20));
+        if (cudaMallocHost(&pinned[slot], want) != cudaSuccess) {
+            cudaGetLastError();
+            arena.release(off, f.bytes);
+            lk.lock();
+            fail_front(fail(NBG_ENOMEM, "pinned staging of %zu bytes unavailable", want));
+            return true;
         }
-        f.hstage = pinned[slot];
+        pinned_bytes[slot] = want;
     }
+    char* stage = pinned[slot];
+    const size_t st_in = up256(head), st_out = st_in + host_in;
     slot_busy[slot] = true;
     size_t ho = 0, ro = 0;
-    for (size_t k = 0; k < ids.size(); k++) {
-        Request& q = reqs[ids[k]];
+    for (size_t k = 0; k < in.size(); k++) {
+        if (!host[k]) continue;
+        const ProdIn& q = in[k];
         DProd& P = f.bb.prods[k];
-        if (q.host) {
-            const size_t na = 8 * (size_t)q.in.m;
-            memcpy(f.hstage + ho, q.in.a, na);
-            P.a = (const uint64_t*)(base + dev_in + ho);
-            ho += up256(na);
-            if (q.in.sqr) {
-                P.b = P.a;
-            } else {
-                const size_t nb = 8 * (size_t)q.in.n;
-                memcpy(f.hstage + ho, q.in.b, nb);
-                P.b = (const uint64_t*)(base + dev_in + ho);
-                ho += up256(nb);
-            }
-            P.r = (uint64_t*)(base + dev_out + ro);
-            f.host_results.push_back({host_in + ro, ids[k]});
-            ro += up256(8 * (size_t)(q.in.m + q.in.n));
+        const size_t na = 8 * (size_t)q.m;
+        memcpy(stage + st_in + ho, q.a, na);
+        P.a = (const uint64_t*)(base + dev_in + ho);
+        ho += up256(na);
+        if (q.sqr) {
+            P.b = P.a;
+        } else {
+            const size_t nb = 8 * (size_t)q.n;
+            memcpy(stage + st_in + ho, q.b, nb);
+            P.b = (const uint64_t*)(base + dev_in + ho);
+            ho += up256(nb);
         }
-        q.state = 1;
+        P.r = (uint64_t*)(base + dev_out + ro);
+        f.host_results.push_back({st_out + ro, q.r, 8 * (size_t)(q.m + q.n)});
+        ro += up256(8 * (size_t)(q.m + q.n));
     }
-    bool ok = true;
-    if (host_in) ok = cudaMemcpyAsync(base + dev_in, f.hstage, host_in, cudaMemcpyHostToDevice, f.st) == cudaSuccess;
-    ok = ok && upload_batch(E, f.bb, base, f.st) == NBG_OK;
-    ok = ok && run_launches(E, f.bb, base, f.st) == NBG_OK;
+    bind_batch(f.bb, base);
+    stage_batch(f.bb, stage);
+    bool ok = cudaMemcpyAsync(base, stage, head, cudaMemcpyHostToDevice, f.st) == cudaSuccess;
+    if (ok && host_in)
+        ok = cudaMemcpyAsync(base + dev_in, stage + st_in, host_in, cudaMemcpyHostToDevice, f.st) == cudaSuccess;
+    {
+        std::lock_guard<std::recursive_mutex> elk(E.mu);
+        ok = ok && run_launches_branched(E, f.bb, base, f.st, side[slot], NSIDE) == NBG_OK;
+    }
     if (ok && host_out)
-        ok = cudaMemcpyAsync(f.hstage + host_in, base + dev_out, host_out, cudaMemcpyDeviceToHost, f.st) == cudaSuccess;
+        ok = cudaMemcpyAsync(stage + st_out, base + dev_out, host_out, cudaMemcpyDeviceToHost, f.st) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventRecord(f.done, f.st) == cudaSuccess;
-    for (size_t k = 0; k < ids.size(); k++) pending.pop_front();
-    f.ids = std::move(ids);
+    ok = ok && cudaLaunchHostFunc(f.st, on_batch_done, this) == cudaSuccess;
     if (!ok) {
         // the stream's work is abandoned: fail the batch's requests
         cudaStreamSynchronize(f.st);
-        for (int64_t id : f.ids) {
-            Request& q = reqs[id];
-            q.state = 3;
-            q.rc = NBG_ECUDA;
-            q.t_done = now_us();
-            failed++;
-        }
         if (f.done) cudaEventDestroy(f.done);
         arena.release(f.off, f.bytes);
         slot_busy[f.slot] = false;
-        cv_done.notify_all();
+        lk.lock();
+        for (size_t k = 0; k < ids.size(); k++) fail_front(NBG_ECUDA);
         return true;
     }
+    lk.lock();
+    for (size_t k = 0; k < ids.size(); k++) {
+        Request& q = reqs[ids[k]];
+        q.state = 1;
+        pending_points -= q.points;
+        pending.pop_front();
+    }
+    batches++;
+    batched_requests += (int64_t)ids.size();
+    f.ids = std::move(ids);
     flights.push_back(std::move(f));
-    (void)lk;
     return true;
 }
 
-// Marks finished batches done.  wait_one: block on the oldest if nothing finished.
-void nbg_server::retire(std::unique_lock<std::mutex>& lk, bool wait_one) {
-    bool any = false;
+// Marks finished batches done.  Entered and left with the server lock held; host results are
+// copied out to the callers' buffers with the lock dropped.
+void nbg_server::retire(std::unique_lock<std::mutex>& lk) {
+    std::vector<std::pair<Flight, cudaError_t>> fin;
     for (auto it = flights.begin(); it != flights.end();) {
         cudaError_t q = cudaEventQuery(it->done);
         if (q == cudaErrorNotReady) {
             ++it;
             continue;
         }
-        const double t = now_us();
-        for (const auto& hr : it->host_results) {
-            Request& rq = reqs[hr.second];
-            memcpy(rq.in.r, it->hstage + hr.first, 8 * (size_t)(rq.in.m + rq.in.n));
-        }
-        for (int64_t id : it->ids) {
+        fin.emplace_back(std::move(*it), q);
+        it = flights.erase(it);
+    }
+    if (fin.empty()) return;
+    lk.unlock();
+    const double t = now_us();
+    for (auto& fe : fin) {
+        Flight& fl = fe.first;
+        if (fe.second == cudaSuccess)
+            for (const auto& hr : fl.host_results) memcpy(hr.dst, pinned[fl.slot] + hr.stage_off, hr.bytes);
+        cudaEventDestroy(fl.done);
+        arena.release(fl.off, fl.bytes);
+        slot_busy[fl.slot] = false;
+    }
+    lk.lock();
+    for (auto& fe : fin) {
+        for (int64_t id : fe.first.ids) {
             Request& rq = reqs[id];
-            rq.state = q == cudaSuccess ? 2 : 3;
-            rq.rc = q == cudaSuccess ? NBG_OK : NBG_ECUDA;
+            const bool ok = fe.second == cudaSuccess;
+            rq.state = ok ? 2 : 3;
+            rq.rc = ok ? NBG_OK : NBG_ECUDA;
             rq.t_done = t;
-            if (q == cudaSuccess) {
+            if (ok) {
                 completed++;
                 latencies_us.push_back(t - rq.t_submit);
                 limbs_done += (double)(rq.in.m + rq.in.n);
@@ -306,39 +354,30 @@ void nbg_server::retire(std::unique_lock<std::mutex>& lk, bool wait_one) {
                 failed++;
             }
         }
-        cudaEventDestroy(it->done);
-        arena.release(it->off, it->bytes);
-        slot_busy[it->slot] = false;
-        it = flights.erase(it);
-        any = true;
     }
-    if (any) {
-        cv_done.notify_all();
-        return;
-    }
-    if (wait_one && !flights.empty()) {
-        cudaEvent_t ev = flights.front().done;
-        lk.unlock();
-        cudaEventSynchronize(ev);
-        lk.lock();
-    }
+    cv_done.notify_all();
+}
+
+// Host callback queued behind each batch: wakes the worker to retire it.
+// It takes only the server lock and calls no CUDA function.
+void CUDART_CB nbg_server::on_batch_done(void* self) {
+    nbg_server* s = (nbg_server*)self;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->wake = true;
+    s->cv_work.notify_all();
 }
 
 void nbg_server::run() {
     std::unique_lock<std::mutex> lk(mu);
     while (!stop.load() || !pending.empty() || !flights.empty()) {
-        retire(lk, false);
+        wake = false;
+        retire(lk);
         bool launched = false;
         while (launch_batch(lk)) launched = true;
-        if (launched) continue;
-        if (!flights.empty()) {
-            // a batch slot or memory will free up when the oldest batch ends;
-            // new arrivals also wake us
-            if (pending.empty()) cv_work.wait_for(lk, std::chrono::microseconds(50));
-            else retire(lk, true);
-        } else if (!stop.load()) {
-            cv_work.wait_for(lk, std::chrono::milliseconds(5));
-        }
+        if (launched || wake) continue;  // wake: something happened while the lock was dropped
+        // woken by a submission or a batch's completion callback; the timeout
+        // is only a backstop
+        cv_work.wait_for(lk, std::chrono::milliseconds(flights.empty() ? 5 : 2));
     }
 }
 
@@ -360,7 +399,10 @@ int nbg_server_create(const nbg_server_opts* opts, nbg_server** out) {
         return fail(NBG_ENOMEM, "server arena of %lld bytes unavailable", (long long)opts->hbm_budget_bytes);
     }
     s->arena.reset((size_t)opts->hbm_budget_bytes);
-    for (int i = 0; i < MAX_FLIGHT; i++) cudaStreamCreateWithFlags(&s->streams[i], cudaStreamNonBlocking);
+    for (int i = 0; i < MAX_FLIGHT; i++) {
+        cudaStreamCreateWithFlags(&s->streams[i], cudaStreamNonBlocking);
+        for (int j = 0; j < NSIDE; j++) cudaStreamCreateWithFlags(&s->side[i][j], cudaStreamNonBlocking);
+    }
     s->worker = std::thread([s] { s->run(); });
     *out = s;
     return NBG_OK;
@@ -387,6 +429,12 @@ static int submit(nbg_server* s, const nbg_desc* d, bool host, int64_t* ticket) 
         q.bits_a = d->bits_a;
         q.bits_b = sqr ? d->bits_a : d->bits_b;
     }
+    double points = 0;
+    {
+        int bw = 0;
+        int64_t N = 0;
+        if (ntt_params(q.bits_a, q.bits_b, &bw, &N) == NBG_OK) points = (double)N;
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop.load()) return fail(NBG_EINVAL, "server is stopping");
     if (s->opts.max_queue > 0 && (int64_t)s->pending.size() >= s->opts.max_queue)
@@ -396,6 +444,9 @@ static int submit(nbg_server* s, const nbg_desc* d, bool host, int64_t* ticket) 
     r.in = q;
     r.host = host;
     r.t_submit = now_us();
+    r.points = points;
+    s->pending_points += points;
+    s->wake = true;
     if (s->t_first == 0) s->t_first = r.t_submit;
     s->pending.push_back(id);
     *ticket = id;
@@ -453,6 +504,8 @@ int nbg_server_stats(nbg_server* s, nbg_server_stats_t* st) {
     st->p99_ms = pct(0.99) / 1e3;
     const double span = s->t_last - s->t_first;
     st->output_limbs_per_s = span > 0 ? s->limbs_done / (span * 1e-6) : 0.0;
+    st->batches = s->batches;
+    st->mean_batch_requests = s->batches ? (double)s->batched_requests / (double)s->batches : 0.0;
     return NBG_OK;
 }
 
@@ -465,7 +518,9 @@ int nbg_server_destroy(nbg_server* s) {
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
     for (int i = 0; i < MAX_FLIGHT; i++) {
+        cudaStreamSynchronize(s->streams[i]);  // its completion callbacks included
         cudaStreamDestroy(s->streams[i]);
+        for (int j = 0; j < NSIDE; j++) cudaStreamDestroy(s->side[i][j]);
         if (s->pinned[i]) cudaFreeHost(s->pinned[i]);
     }
     cudaFree(s->dmem);

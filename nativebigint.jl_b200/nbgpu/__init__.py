@@ -291,21 +291,24 @@ class Batch:
 # serving (continuous batching)
 
 class ServerOpts(ctypes.Structure):
-    _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("max_batch", ctypes.c_int64), ("max_queue", ctypes.c_int64)]
+    _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("max_batch", ctypes.c_int64), ("max_queue", ctypes.c_int64),
+                ("batch_points", ctypes.c_int64)]
 
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("pending", ctypes.c_int64),
                 ("in_flight_batches", ctypes.c_int32), ("reserved", ctypes.c_int32), ("p50_ms", ctypes.c_double),
-                ("p99_ms", ctypes.c_double), ("output_limbs_per_s", ctypes.c_double)]
+                ("p99_ms", ctypes.c_double), ("output_limbs_per_s", ctypes.c_double), ("batches", ctypes.c_int64),
+                ("mean_batch_requests", ctypes.c_double)]
 
 
 class Server:
     """Continuous-batching product server (nbg_server_*)."""
 
-    def __init__(self, hbm_budget_bytes: int = 1 << 30, max_batch: int = 0, max_queue: int = 0):
+    def __init__(self, hbm_budget_bytes: int = 1 << 30, max_batch: int = 0, max_queue: int = 0,
+                 batch_points: int = 0):
         self._h = ctypes.c_void_p()
-        opts = ServerOpts(hbm_budget_bytes, max_batch, max_queue)
+        opts = ServerOpts(hbm_budget_bytes, max_batch, max_queue, batch_points)
         _check(lib().nbg_server_create(ctypes.byref(opts), ctypes.byref(self._h)))
         self._keep: dict = {}
 

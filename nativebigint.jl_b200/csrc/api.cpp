@@ -394,7 +394,7 @@ int transform_passes(double* x, int64_t N, int prime, bool fwd, cudaStream_t st)
     CUDA_TRY(cudaMemcpyAsync(d, &P, sizeof P, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(d + jo, jobs.data(), sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, st));
     for (const Launch& L : ls) {
-        CUDA_TRY(launch_jobs(L.kind, (const DProd*)d, E.d_plans, (const Job*)(d + jo) + L.off, L.n, L.smem, 0, st));
+        CUDA_TRY(launch_jobs(L.kind, (const DProd*)d, E.d_plans, job_list((const Job*)(d + jo) + L.off), L.n, L.smem, 0, st));
         g_launches++;
     }
     CUDA_TRY(cudaStreamSynchronize(st));
@@ -594,12 +594,13 @@ int nbg_batch_profile(nbg_batch* bt, void* stream, float* ms, int32_t cap) {
     std::vector<cudaEvent_t> ev(ls.size() + 1);
     for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
     const DProd* prods = (const DProd*)(bt->dmem + bt->bb.off_prods);
-    const Job* jobs = (const Job*)(bt->dmem + bt->bb.off_jobs);
+    const Job* jobs = (const Job*)(bt->dmem + bt->bb.off_joblist);
+    CUDA_TRY(expand_jobs(bt->bb, bt->dmem, st));
     int rc = NBG_OK;
     CUDA_TRY(cudaEventRecord(ev[0], st));
     for (size_t i = 0; i < ls.size(); i++) {
         const Launch& L = ls[i];
-        cudaError_t e = launch_jobs(L.kind, prods, g_eng.d_plans, jobs + L.off, L.n, L.smem, 0, st);
+        cudaError_t e = launch_jobs(L.kind, prods, g_eng.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st);
         if (e != cudaSuccess) { rc = fail(NBG_ECUDA, "profile launch: %s", cudaGetErrorString(e)); break; }
         g_launches++;
         CUDA_TRY(cudaEventRecord(ev[i + 1], st));
@@ -703,9 +704,9 @@ int nbg_unpack_dev(uint64_t* r, int64_t rn, const double* x1, const double* x2, 
     CUDA_TRY(cudaMemcpyAsync(d, &P, sizeof P, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(d + jo, jobs.data(), sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, st));
     const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / b + 4;
-    CUDA_TRY(launch_jobs(JK_UNPACK, (const DProd*)d, E.d_plans, (const Job*)(d + jo), P.ntl,
+    CUDA_TRY(launch_jobs(JK_UNPACK, (const DProd*)d, E.d_plans, job_list((const Job*)(d + jo)), P.ntl,
                          sizeof(uint64_t) * 2 * align_up((size_t)ncoef, 2), 0, st));
-    CUDA_TRY(launch_jobs(JK_CARRY, (const DProd*)d, E.d_plans, (const Job*)(d + jo) + P.ntl, 1, 0, 0, st));
+    CUDA_TRY(launch_jobs(JK_CARRY, (const DProd*)d, E.d_plans, job_list((const Job*)(d + jo) + P.ntl), 1, 0, 0, st));
     g_launches += 2;
     CUDA_TRY(cudaStreamSynchronize(st));
     return NBG_OK;

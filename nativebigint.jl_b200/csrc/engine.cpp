@@ -752,7 +752,10 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         return o;
     };
     struct Group {
-        std::vector<Job> jobs;
+        std::vector<JobSeg> segs;
+        std::vector<int32_t> plist;
+        int64_t njobs = 0;
+        int mode = JM_SEGS;
         double ops = 0, bytes = 0;
     };
     // key: (step order, kind, smem)
@@ -790,9 +793,16 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         const int nop = P0.sqr ? 1 : 2;
         const double nc = (double)cls.size();
         auto emit = [&](Group& g, const DPass& ps, int nopnd, int sub_base) {
-            for (int64_t t = 0; t < ps.ntiles; t++)
-                for (int op = 0; op < nopnd; op++)
-                    for (int32_t k : cls) g.jobs.push_back(Job{k, sub_base | (op << 1), t});
+            JobSeg sg;
+            sg.begin = g.njobs;
+            sg.ntiles = ps.ntiles;
+            sg.nop = nopnd;
+            sg.nprod = (int32_t)cls.size();
+            sg.first = (int32_t)g.plist.size();
+            sg.sub_base = sub_base;
+            g.segs.push_back(sg);
+            g.plist.insert(g.plist.end(), cls.begin(), cls.end());
+            g.njobs += ps.ntiles * nopnd * (int64_t)cls.size();
         };
         for (int p = 0; p < Pn - 1; p++) {
             const DPass& ps = pl.pass[p];
@@ -830,38 +840,73 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
     }
     const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / bmin + 4;
     const size_t unp_smem = sizeof(uint64_t) * 2 * (size_t)align_up((size_t)ncoef, 2);
+    // unpack: product k owns tiles [agg_off[k], agg_off[k] + ntl); carry: one CTA per product
     Group& gu = group_of(2 * pmax - 1, JK_UNPACK, unp_smem);
+    gu.mode = JM_TILES;
+    gu.njobs = (int64_t)aggw;
+    bool any_carry = false;
+    double carry_bytes = 0;
     for (int64_t k = 0; k < count; k++) {
         const DProd& P = bb.prods[(size_t)k];
-        for (int64_t t = 0; t < P.ntl; t++) gu.jobs.push_back(Job{(int32_t)k, 0, t});
         gu.ops += 28.0 * (double)P.nconv;
         gu.bytes += 16.0 * (double)P.nconv + 8.0 * (double)P.rn;
         if (P.ntl > 1) {
-            Group& gc = group_of(2 * pmax, JK_CARRY, 0);
-            gc.jobs.push_back(Job{(int32_t)k, 0, 0});
-            gc.bytes += 4.0 * (double)P.ntl;
+            any_carry = true;
+            carry_bytes += 4.0 * (double)P.ntl;
         }
     }
-    size_t total_jobs = 0;
-    for (auto& kv : groups) total_jobs += kv.second.jobs.size();
-    bb.jobs.reserve(total_jobs);
+    if (any_carry) {
+        Group& gc = group_of(2 * pmax, JK_CARRY, 0);
+        gc.mode = JM_PERPROD;
+        gc.njobs = count;
+        gc.bytes = carry_bytes;
+    }
+    // job table: [segments | product list] per launch, then the unpack tile starts
+    size_t tb = 0;
     for (auto& kv : groups) {
+        const Group& g = kv.second;
         const int kind = std::get<1>(kv.first);
-        std::vector<Job>& v = kv.second.jobs;
-        Launch L{kind, (int64_t)bb.jobs.size(), (int64_t)v.size(), std::get<2>(kv.first)};
+        Launch L{kind, bb.total_jobs, g.njobs, std::get<2>(kv.first)};
+        bb.total_jobs += g.njobs;
         L.step = std::get<0>(kv.first);
-        L.alg_ops = kv.second.ops;
-        L.alg_bytes = kv.second.bytes;
+        L.alg_ops = g.ops;
+        L.alg_bytes = g.bytes;
+        L.mode = g.mode;
         if ((int)L.smem > E.smem_optin) return fail(NBG_EINVAL, "tile needs %zu bytes of shared memory", L.smem);
+        if (g.mode == JM_SEGS) {
+            L.nseg = (int)g.segs.size();
+            L.seg_off = tb;
+            tb = align_up(tb + sizeof(JobSeg) * g.segs.size(), 16);
+            L.plist_off = tb;
+            tb = align_up(tb + sizeof(int32_t) * g.plist.size(), 16);
+        }
         bb.launches.push_back(L);
-        bb.jobs.insert(bb.jobs.end(), v.begin(), v.end());
-        std::vector<Job>().swap(v);
+    }
+    bb.tstart_off = tb;
+    tb = align_up(tb + sizeof(int64_t) * ((size_t)count + 1), 16);
+    bb.expand_off = tb;
+    tb = align_up(tb + sizeof(ExpandEntry) * bb.launches.size(), 16);
+    bb.table.assign(tb, 0);
+    {
+        size_t li = 0;
+        for (auto& kv : groups) {
+            const Group& g = kv.second;
+            const Launch& L = bb.launches[li++];
+            if (g.mode != JM_SEGS) continue;
+            memcpy(bb.table.data() + L.seg_off, g.segs.data(), sizeof(JobSeg) * g.segs.size());
+            memcpy(bb.table.data() + L.plist_off, g.plist.data(), sizeof(int32_t) * g.plist.size());
+        }
+        int64_t* ts = (int64_t*)(bb.table.data() + bb.tstart_off);
+        for (int64_t k = 0; k < count; k++) ts[k] = (int64_t)agg_off[(size_t)k];
+        ts[count] = (int64_t)aggw;
     }
 
     // device layout: [prods | jobs | work | agg]
     bb.off_prods = 0;
     bb.off_jobs = align_up(sizeof(DProd) * (size_t)count, 256);
-    bb.off_work = align_up(bb.off_jobs + sizeof(Job) * bb.jobs.size(), 256);
+    bb.head_bytes = bb.off_jobs + bb.table.size();
+    bb.off_joblist = align_up(bb.head_bytes, 256);
+    bb.off_work = align_up(bb.off_joblist + sizeof(Job) * (size_t)bb.total_jobs, 256);
     bb.off_agg = align_up(bb.off_work + sizeof(double) * work, 256);
     bb.dev_bytes = align_up(bb.off_agg + sizeof(uint32_t) * aggw, 256);
     return NBG_OK;
@@ -883,31 +928,56 @@ void bind_batch(BatchBuild& bb, char* dbase) {
         }
         P.agg = agg + bb.agg_off[k];
     }
+    ExpandEntry* ex = (ExpandEntry*)(bb.table.data() + bb.expand_off);
+    for (size_t i = 0; i < bb.launches.size(); i++) {
+        ex[i].src = launch_src(bb, bb.launches[i], dbase);
+        ex[i].begin = bb.launches[i].off;
+        ex[i].n = bb.launches[i].n;
+    }
 }
 
 void stage_batch(const BatchBuild& bb, char* host) {
-    memset(host, 0, bb.off_work);
+    memset(host, 0, bb.head_bytes);
     memcpy(host + bb.off_prods, bb.prods.data(), sizeof(DProd) * bb.prods.size());
-    if (!bb.jobs.empty()) memcpy(host + bb.off_jobs, bb.jobs.data(), sizeof(Job) * bb.jobs.size());
+    if (!bb.table.empty()) memcpy(host + bb.off_jobs, bb.table.data(), bb.table.size());
 }
 
-// Point the descriptors at the device block and upload descriptors + jobs.
+JobSrc launch_src(const BatchBuild& bb, const Launch& L, const char* dbase) {
+    JobSrc s{};
+    const char* t = dbase + bb.off_jobs;
+    s.mode = L.mode;
+    s.segs = (const JobSeg*)(t + L.seg_off);
+    s.nseg = L.nseg;
+    s.plist = (const int32_t*)(t + L.plist_off);
+    s.tstart = (const int64_t*)(t + bb.tstart_off);
+    s.nprod = (int64_t)bb.prods.size();
+    return s;
+}
+
+// Point the descriptors at the device block and upload descriptors + job table.
 int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st) {
     bind_batch(bb, dbase);
     CUDA_TRY(cudaMemcpyAsync(dbase + bb.off_prods, bb.prods.data(), sizeof(DProd) * bb.prods.size(),
                              cudaMemcpyHostToDevice, st));
-    if (!bb.jobs.empty())
-        CUDA_TRY(cudaMemcpyAsync(dbase + bb.off_jobs, bb.jobs.data(), sizeof(Job) * bb.jobs.size(),
+    if (!bb.table.empty())
+        CUDA_TRY(cudaMemcpyAsync(dbase + bb.off_jobs, bb.table.data(), bb.table.size(),
                                  cudaMemcpyHostToDevice, st));
     (void)E;
     return NBG_OK;
 }
 
+cudaError_t expand_jobs(const BatchBuild& bb, char* dbase, cudaStream_t st) {
+    return launch_expand((const ExpandEntry*)(dbase + bb.off_jobs + bb.expand_off), (int)bb.launches.size(),
+                         (Job*)(dbase + bb.off_joblist), bb.total_jobs, st);
+}
+
 int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st) {
     const DProd* prods = (const DProd*)(dbase + bb.off_prods);
-    const Job* jobs = (const Job*)(dbase + bb.off_jobs);
+    const Job* jobs = (const Job*)(dbase + bb.off_joblist);
+    CUDA_TRY(expand_jobs(bb, dbase, st));
+    g_launches++;
     for (const Launch& L : bb.launches) {
-        cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, jobs + L.off, L.n, L.smem, 0, st);
+        cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st);
         if (e != cudaSuccess) return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n,
                                           cudaGetErrorString(e));
         g_launches++;
@@ -918,7 +988,9 @@ int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st) 
 int run_launches_branched(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, cudaStream_t* side,
                           int nside) {
     const DProd* prods = (const DProd*)(dbase + bb.off_prods);
-    const Job* jobs = (const Job*)(dbase + bb.off_jobs);
+    const Job* jobs = (const Job*)(dbase + bb.off_joblist);
+    CUDA_TRY(expand_jobs(bb, dbase, st));
+    g_launches++;
     size_t i = 0;
     while (i < bb.launches.size()) {
         size_t j = i;
@@ -937,7 +1009,7 @@ int run_launches_branched(Engine& E, const BatchBuild& bb, char* dbase, cudaStre
                 s = side[(k - i - 1) % (size_t)nside];
                 CUDA_TRY(cudaStreamWaitEvent(s, fork, 0));
             }
-            cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, jobs + L.off, L.n, L.smem, 0, s);
+            cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, s);
             if (e != cudaSuccess)
                 return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n, cudaGetErrorString(e));
             g_launches++;

@@ -96,8 +96,13 @@ struct ProdIn {
 
 struct Launch {
     int kind;
-    int64_t off, n;
+    int64_t off, n;        // explicit lists: first job and count; batches: n = job count
     size_t smem;
+    // batches: where the launch's jobs are described (JobMode), as byte
+    // offsets into the batch's job table
+    int mode = JM_LIST;
+    int nseg = 0;
+    size_t seg_off = 0, plist_off = 0;
     int step = 0;          // pipeline step: launches of one step are independent
     double alg_ops = 0;    // FP64 instructions of the reference schedule done by this launch
     double alg_bytes = 0;  // compulsory global bytes (operand/limb reads, tile loads and stores)
@@ -106,7 +111,12 @@ struct Launch {
 struct BatchBuild {
     std::vector<DProd> prods;
     std::vector<PlanRec*> plan_of;
-    std::vector<Job> jobs;
+    std::vector<char> table;  // job table: per launch segments and product lists, then tile starts
+    size_t tstart_off = 0;    // per-product first unpack tile (count + 1 int64), in the table
+    size_t expand_off = 0;    // ExpandEntry per launch, in the table (written by bind_batch)
+    int64_t total_jobs = 0;   // explicit jobs, written on the device by the expansion kernel
+    size_t off_joblist = 0;   // region offset of that job list
+    size_t head_bytes = 0;    // [0, head_bytes): descriptors and table, the host-written head
     std::vector<Launch> launches;
     std::vector<size_t> xa_off, xb_off, agg_off;
     size_t work_doubles = 0, agg_words = 0;
@@ -118,9 +128,14 @@ int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st);
 // Points each product's workspace and carry words into the batch's device
 // region at dbase (what upload_batch does before copying).
 void bind_batch(BatchBuild& bb, char* dbase);
-// Writes the bound descriptors and job list into `host` in their device
-// layout: off_work bytes that one copy to dbase makes the region's head.
+// Writes the bound descriptors and job table into `host` in their device
+// layout: head_bytes that one copy to dbase makes the region's head.
 void stage_batch(const BatchBuild& bb, char* host);
+// Writes the batch's explicit job list on the device (one kernel); the
+// run_launches functions do this before the batch's first launch.
+cudaError_t expand_jobs(const BatchBuild& bb, char* dbase, cudaStream_t st);
+// The job source of launch L of a batch whose region starts at dbase.
+JobSrc launch_src(const BatchBuild& bb, const Launch& L, const char* dbase);
 int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st);
 // Same, with the independent launches of each step forked onto `side`
 // streams (used while capturing a CUDA graph, where they become parallel branches).

@@ -541,10 +541,10 @@ __device__ __forceinline__ Tiles make_tiles(double* s, int stride, int ntiles, i
 // Forward pass of one tile of one operand, both primes (tiles X0, X1).
 __global__ void __launch_bounds__(PASS_THREADS, NBG_COL_MINB) k_fwd(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
-                                                         const Job* __restrict__ jobs, int64_t njobs) {
+                                                         const JobSrc src, int64_t njobs) {
     extern __shared__ double smem[];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const Job jb = jobs[ji];
+        const Job jb = job_at(src, ji);
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int opb = (jb.sub >> 1) & 1, pass = (jb.sub >> 8) & 0xff;
@@ -575,10 +575,10 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_COL_MINB) k_fwd(const DProd*
 // Tiles: products [a0, b0, a1, b1], squares [a0, a1].
 __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
-                                                         const Job* __restrict__ jobs, int64_t njobs) {
+                                                         const JobSrc src, int64_t njobs) {
     extern __shared__ double smem[];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const Job jb = jobs[ji];
+        const Job jb = job_at(src, ji);
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int pass = P.npass - 1;
@@ -644,10 +644,10 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
 // Reverse pass of one tile, both primes.
 __global__ void __launch_bounds__(PASS_THREADS, NBG_COL_MINB) k_rev(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
-                                                         const Job* __restrict__ jobs, int64_t njobs) {
+                                                         const JobSrc src, int64_t njobs) {
     extern __shared__ double smem[];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const Job jb = jobs[ji];
+        const Job jb = job_at(src, ji);
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int pass = (jb.sub >> 8) & 0xff;
@@ -747,12 +747,12 @@ __device__ __forceinline__ void limb_range(int64_t w, int b, double rb, int64_t 
 
 __global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restrict__ prods,
                                                            const DPlan* __restrict__ plans,
-                                                           const Job* __restrict__ jobs, int64_t njobs) {
+                                                           const JobSrc src, int64_t njobs) {
     extern __shared__ uint64_t usm[];
     __shared__ uint32_t wagg[UNPACK_THREADS / 32];
     __shared__ uint64_t hilast[UNPACK_THREADS + 1];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const Job jb = jobs[ji];
+        const Job jb = job_at(src, ji);
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int b = P.bch;
@@ -858,12 +858,13 @@ __global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restri
 // Cross-tile carries: one CTA per product.  Each thread composes a run of
 // tile aggregates, the block scans them, and every tile whose true carry-in is
 // 1 gets +1 propagated from its first limb (limbs equal to 2^64-1 wrap to 0).
-__global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, const Job* __restrict__ jobs,
+__global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, const JobSrc src,
                                                int64_t njobs) {
     __shared__ uint32_t wagg[8];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const DProd& P = prods[jobs[ji].prod];
+        const DProd& P = prods[job_at(src, ji).prod];
         const int64_t nt = P.ntl;
+        if (nt <= 1) continue;  // one tile: no carry crosses a tile boundary
         const int t = threadIdx.x;
         const int64_t per = (nt + blockDim.x - 1) / blockDim.x;
         const int64_t t0 = (int64_t)t * per, t1 = min(t0 + per, nt);
@@ -980,7 +981,7 @@ cudaError_t kernels_init(double p1, double p2) {
 
 int kernels_smem_optin() { return g_smem_optin; }
 
-cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const Job* jobs, int64_t njobs,
+cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& jobs, int64_t njobs,
                         size_t smem, int grid_cap, cudaStream_t st) {
     if (njobs <= 0) return cudaSuccess;
     int64_t grid64 = njobs;
@@ -995,6 +996,29 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
         case JK_CARRY: k_carry<<<grid, 256, 0, st>>>(prods, jobs, njobs); break;
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+// One thread per job: find the launch owning job g, decode it, store it.
+__global__ void __launch_bounds__(256) k_expand(const ExpandEntry* __restrict__ entries, int nentries,
+                                                Job* __restrict__ out, int64_t total) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nentries - 1;  // last entry with begin <= g
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (entries[mid].begin <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        out[g] = job_at(entries[lo].src, g - entries[lo].begin);
+    }
+}
+
+cudaError_t launch_expand(const ExpandEntry* entries, int nentries, Job* out, int64_t total, cudaStream_t st) {
+    if (total <= 0 || nentries <= 0) return cudaSuccess;
+    int64_t b = (total + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    k_expand<<<(unsigned)b, 256, 0, st>>>(entries, nentries, out, total);
     return cudaGetLastError();
 }
 

@@ -10,9 +10,21 @@ namespace nbg {
 cudaError_t kernels_init(double p1, double p2);
 int kernels_smem_optin();
 
-// One work-queue launch of `kind` (JobKind) over jobs[0..njobs).
-cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const Job* jobs, int64_t njobs,
+// An explicit job list as a launch's job source.
+inline JobSrc job_list(const Job* l) {
+    JobSrc s{};
+    s.list = l;
+    s.mode = JM_LIST;
+    return s;
+}
+
+// One work-queue launch of `kind` (JobKind) over jobs 0..njobs-1 of `jobs`.
+cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& jobs, int64_t njobs,
                         size_t smem, int grid_cap, cudaStream_t st);
+
+// Writes a batch's explicit job list from its compact description: out[g] for
+// every g < total, entry e covering [e.begin, e.begin + e.n).
+cudaError_t launch_expand(const ExpandEntry* entries, int nentries, Job* out, int64_t total, cudaStream_t st);
 
 // Expands one stage's twiddle table (see k_twiddle).
 cudaError_t launch_twiddle(double* out, int m, int64_t Q, int64_t step, const double* hi, const double* lo, int f,

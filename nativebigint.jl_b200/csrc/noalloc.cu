@@ -283,7 +283,7 @@ extern "C" int nbg_mul_dev_noalloc(uint64_t* r, const uint64_t* a, int64_t m, co
         return cudaGetLastError();
     };
     auto run = [&](int kind, int64_t cnt, size_t smem) -> cudaError_t {
-        cudaError_t e = launch_jobs(kind, dprod, dplan, jobs + jo, cnt, smem, 0, st);
+        cudaError_t e = launch_jobs(kind, dprod, dplan, job_list(jobs + jo), cnt, smem, 0, st);
         jo += cnt;
         return e;
     };

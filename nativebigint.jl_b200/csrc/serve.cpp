@@ -234,7 +234,7 @@ bool nbg_server::launch_batch(std::unique_lock<std::mutex>& lk) {
     f.st = streams[slot];
     // The slot's pinned buffer holds [descriptors and jobs | host operands |
     // host results]; descriptors and operands go over in one copy each.
-    const size_t head = f.bb.off_work;
+    const size_t head = f.bb.head_bytes;
     const size_t dev_in = up256(f.bb.dev_bytes), dev_out = dev_in + host_in;
     const size_t need = up256(head) + host_in + host_out;
     if (pinned_bytes[slot] < need) {

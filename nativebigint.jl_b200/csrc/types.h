@@ -92,6 +92,81 @@ struct Job {
     int64_t tile;
 };
 
+// A run of jobs of one plan class inside a launch: jobs [begin, begin +
+// ntiles * nop * nprod), ordered tile-major, then operand, then product, so
+// CTAs that run together read the same twiddle slice.  The class's products
+// are plist[first .. first + nprod).
+struct JobSeg {
+    int64_t begin;
+    int64_t ntiles;
+    int32_t nop, nprod;
+    int32_t first, sub_base;
+};
+
+// Where a launch's jobs come from.  Batches describe them implicitly, so the
+// host writes a few bytes per plan class or product instead of one Job per CTA.
+enum JobMode : int32_t {
+    JM_LIST = 0,     // list[ji]
+    JM_SEGS = 1,     // segs[nseg] over plist
+    JM_TILES = 2,    // product k owns jobs [tstart[k], tstart[k+1]): tile = ji - tstart[k]
+    JM_PERPROD = 3,  // job ji is product ji, tile 0
+};
+struct JobSrc {
+    const Job* list;
+    const JobSeg* segs;
+    const int32_t* plist;
+    const int64_t* tstart;
+    int32_t mode, nseg;
+    int64_t nprod;  // JM_TILES: products in tstart (tstart has nprod + 1 entries)
+};
+
+// One launch of a batch for the job-expansion kernel: jobs [begin, begin + n)
+// of the batch's job list are jobs 0..n-1 of src.
+struct ExpandEntry {
+    JobSrc src;
+    int64_t begin, n;
+};
+
+// Job ji of a launch described by s (ji < the launch's job count).
+NBG_HD inline Job job_at(const JobSrc& s, int64_t ji) {
+    Job j;
+    if (s.mode == JM_LIST) return s.list[ji];
+    if (s.mode == JM_PERPROD) {
+        j.prod = (int32_t)ji;
+        j.sub = 0;
+        j.tile = 0;
+        return j;
+    }
+    if (s.mode == JM_TILES) {  // last k with tstart[k] <= ji
+        int64_t lo = 0, hi = s.nprod - 1;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) >> 1;
+            if (s.tstart[mid] <= ji) lo = mid;
+            else hi = mid - 1;
+        }
+        j.prod = (int32_t)lo;
+        j.sub = 0;
+        j.tile = ji - s.tstart[lo];
+        return j;
+    }
+    int lo = 0, hi = s.nseg - 1;  // last segment with begin <= ji
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s.segs[mid].begin <= ji) lo = mid;
+        else hi = mid - 1;
+    }
+    const JobSeg g = s.segs[lo];
+    const int64_t local = ji - g.begin;
+    const int64_t per_tile = (int64_t)g.nop * g.nprod;
+    const int64_t t = local / per_tile;
+    const int64_t r = local - t * per_tile;
+    const int32_t op = (int32_t)(r / g.nprod);
+    j.prod = s.plist[g.first + (int32_t)(r - (int64_t)op * g.nprod)];
+    j.sub = g.sub_base | (op << 1);
+    j.tile = t;
+    return j;
+}
+
 enum JobKind : int32_t {
     JK_FWD = 0,   // forward pass (pass 0 packs limbs on load)
     JK_PWR = 1,   // last pass: forward, pointwise, reverse (packs when npass == 1)

@@ -158,6 +158,42 @@ int nbg_server_stats(nbg_server *s, nbg_server_stats_t *st);
 /* Drains the queue, stops the worker, frees the arena. */
 int nbg_server_destroy(nbg_server *s);
 
+/* ---- Barrett powermod chains ------------------------------------------------ */
+
+/* One chain: r[0..k) = b^e mod m.  m has k limbs with m[k-1] != 0 and m > 1;
+ * b has lb <= k limbs (any value, reduced mod m first); e has le limbs and is
+ * nonzero.  The schedule is the reference's powermod_limbs
+ * (src/algorithms.jl:17-107) on its Barrett branch (src/barrett.jl:33-81):
+ * sliding window of width w(bits of e), a table of the odd powers b^1..b^(2^w-1),
+ * and every multiply or square followed by barrett_reduce!. */
+typedef struct nbg_powmod_desc {
+    uint64_t *r;
+    const uint64_t *b;
+    const uint64_t *e;
+    const uint64_t *m;
+    int64_t lb, le;
+} nbg_powmod_desc;
+
+/* count chains sharing one modulus size k, run side by side on the GPU: each
+ * exponent step is one square or multiply per chain plus the two Barrett
+ * products, all three as batched fp-NTT products, the step captured in a CUDA
+ * graph, the chains' state resident on the device.  Host buffers. */
+int nbg_powermod_batch(const nbg_powmod_desc *d, int64_t count, int64_t k);
+/* Same with device buffers (r, b, e, m device pointers), on `stream`; returns
+ * after the work is queued (μ is computed on the host from a copy of m). */
+int nbg_powermod_batch_dev(const nbg_powmod_desc *d, int64_t count, int64_t k, void *stream);
+/* μ = floor(β^(2k) / m), β = 2^64, into mu[0..k+2); returns its normalized
+ * length (k+1, or k+2 iff m = β^(k-1)), or -NBG_EINVAL when m[k-1] = 0.
+ * Host only (barrett_mu!, src/barrett.jl:22-31). */
+int64_t nbg_barrett_mu(const uint64_t *m, int64_t k, uint64_t *mu);
+/* The chain's step list: ops[3*i .. 3*i+2] = (dst, src1, src2) slot indices,
+ * slots 0..T-1 the odd-power table (T = 2^(w-1)), T = b^2, T+1 = accumulator,
+ * T+2 = the raw base, T+3 = the constant 1; src2 = 255 marks a copy of src1.
+ * Returns the number of steps, writing the first min(steps, cap) of them,
+ * or -NBG_EINVAL for a zero exponent; the table size goes to *tsize.
+ * Host only. */
+int64_t nbg_powmod_schedule(const uint64_t *e, int64_t le, uint8_t *ops, int64_t cap, int32_t *tsize);
+
 /* ---- admission (host-side restatement of the reference's sizing) -------- */
 
 /* fp_ntt_params (src/fpntt.jl:964-977): chunk width b and transform length N. */

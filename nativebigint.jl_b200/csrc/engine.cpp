@@ -971,11 +971,13 @@ cudaError_t expand_jobs(const BatchBuild& bb, char* dbase, cudaStream_t st) {
                          (Job*)(dbase + bb.off_joblist), bb.total_jobs, st);
 }
 
-int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st) {
+int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, bool expand) {
     const DProd* prods = (const DProd*)(dbase + bb.off_prods);
     const Job* jobs = (const Job*)(dbase + bb.off_joblist);
-    CUDA_TRY(expand_jobs(bb, dbase, st));
-    g_launches++;
+    if (expand) {
+        CUDA_TRY(expand_jobs(bb, dbase, st));
+        g_launches++;
+    }
     for (const Launch& L : bb.launches) {
         cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st);
         if (e != cudaSuccess) return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n,

@@ -136,7 +136,8 @@ void stage_batch(const BatchBuild& bb, char* host);
 cudaError_t expand_jobs(const BatchBuild& bb, char* dbase, cudaStream_t st);
 // The job source of launch L of a batch whose region starts at dbase.
 JobSrc launch_src(const BatchBuild& bb, const Launch& L, const char* dbase);
-int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st);
+// expand = false reuses the job list a previous run wrote (same region).
+int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, bool expand = true);
 // Same, with the independent launches of each step forked onto `side`
 // streams (used while capturing a CUDA graph, where they become parallel branches).
 int run_launches_branched(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, cudaStream_t* side,

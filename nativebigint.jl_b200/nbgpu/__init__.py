@@ -38,6 +38,7 @@ EXPORTS = [
     "nbg_mul_dev_noalloc", "nbg_load_tuning", "nbg_version", "nbg_trim_plans",
     "nbg_server_create", "nbg_submit", "nbg_submit_dev", "nbg_poll", "nbg_wait", "nbg_release",
     "nbg_server_stats", "nbg_server_destroy",
+    "nbg_powermod_batch", "nbg_powermod_batch_dev", "nbg_barrett_mu", "nbg_powmod_schedule",
 ]
 
 
@@ -104,6 +105,8 @@ def lib() -> ctypes.CDLL:
             "nbg_server_stats": [vp, vp],
             "nbg_server_destroy": [vp],
             "nbg_load_tuning": [c.c_char_p],
+            "nbg_powermod_batch": [vp, i64, i64],
+            "nbg_powermod_batch_dev": [vp, i64, i64, vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -119,6 +122,10 @@ def lib() -> ctypes.CDLL:
         L.nbg_trim_plans.restype = c.c_int
         L.nbg_version.argtypes = []
         L.nbg_version.restype = c.c_char_p
+        L.nbg_barrett_mu.argtypes = [vp, i64, vp]
+        L.nbg_barrett_mu.restype = i64
+        L.nbg_powmod_schedule.argtypes = [vp, i64, vp, i64, c.POINTER(i32)]
+        L.nbg_powmod_schedule.restype = i64
         L.nbg_launch_count.argtypes = []
         L.nbg_launch_count.restype = i64
         _lib = L
@@ -354,6 +361,60 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Barrett powermod chains
+
+class PowmodDesc(ctypes.Structure):
+    _fields_ = [("r", ctypes.c_void_p), ("b", ctypes.c_void_p), ("e", ctypes.c_void_p), ("m", ctypes.c_void_p),
+                ("lb", ctypes.c_int64), ("le", ctypes.c_int64)]
+
+
+def powermod_batch(bases, exps, mods) -> list[np.ndarray]:
+    """r_c = b_c^e_c mod m_c for chains of one modulus size k (limb arrays,
+    host memory); every chain's square/multiply and both Barrett products run
+    as batched GPU products (nbg_powermod_batch)."""
+    mods = [_u64(m) for m in mods]
+    bases = [_u64(b) for b in bases]
+    exps = [_u64(e) for e in exps]
+    k = mods[0].size
+    if any(m.size != k for m in mods):
+        raise ValueError("all moduli need the same limb count")
+    outs = [np.zeros(k, dtype=np.uint64) for _ in mods]
+    d = (PowmodDesc * len(mods))()
+    for i, (r, b, e, m) in enumerate(zip(outs, bases, exps, mods)):
+        d[i] = PowmodDesc(_ptr(r), _ptr(b), _ptr(e), _ptr(m), b.size, e.size)
+    _check(lib().nbg_powermod_batch(ctypes.cast(d, ctypes.c_void_p), len(mods), k))
+    return outs
+
+
+def powermod_batch_dev(descs, k: int, stream=None) -> None:
+    """Device-buffer form: descs is a PowmodDesc array of device pointers."""
+    _check(lib().nbg_powermod_batch_dev(ctypes.cast(descs, ctypes.c_void_p), len(descs), k, _stream(stream)))
+
+
+def barrett_mu(m) -> np.ndarray:
+    """mu = floor(2^(128k) / m) (k + 2 limbs, host computation)."""
+    m = _u64(m)
+    mu = np.zeros(m.size + 2, dtype=np.uint64)
+    n = lib().nbg_barrett_mu(_ptr(m), m.size, _ptr(mu))
+    if n < 0:
+        _check(int(-n))
+    return mu
+
+
+def powmod_schedule(e) -> tuple[np.ndarray, int]:
+    """The chain's step list as an (S, 3) uint8 array (dst, src1, src2) and
+    the odd-power table size."""
+    e = _u64(e)
+    T = ctypes.c_int32()
+    n = lib().nbg_powmod_schedule(_ptr(e), e.size, None, 0, ctypes.byref(T))
+    if n < 0:
+        _check(int(-n))
+    ops = np.zeros((n, 3), dtype=np.uint8)
+    lib().nbg_powmod_schedule(_ptr(e), e.size, ops.ctypes.data, n, ctypes.byref(T))
+    return ops, T.value
 
 
 # ---------------------------------------------------------------------------

@@ -604,6 +604,105 @@ def run_serve(args) -> None:
             raise SystemExit(f"serve: {mismatches} mismatches, {st['failed']} failed at rate {rate}")
 
 
+POWMOD_WORKLOAD = ("Barrett powermod chains: 256-limb odd and even moduli (alternating), 256-limb bases, "
+                   "4096-bit exponents, uniform random limbs")
+
+
+def run_powmod(args) -> None:
+    """Chains of b^e mod m run side by side: each exponent step is one square or
+    multiply per chain plus the two Barrett products, batched across chains.
+    One bench step = one nbg_powermod_batch_dev call over all chains (device
+    buffers); e2e = the same through nbg_powermod_batch with host buffers."""
+    import torch
+
+    import nbgpu
+    import oracle
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    nbgpu._check(nbgpu.lib().nbg_init(dev))
+    rng = np.random.Generator(np.random.PCG64(args.seed))
+    n, k, le = args.powmod_chains, 256, max(1, args.powmod_ebits // 64)
+    mods, bases, exps = [], [], []
+    for i in range(n):
+        m = rng.integers(0, 2**64, k, dtype=np.uint64)
+        m[-1] |= np.uint64(1)
+        m[0] = (m[0] | np.uint64(1)) if i % 2 else (m[0] & ~np.uint64(1))
+        e = rng.integers(0, 2**64, le, dtype=np.uint64)
+        e[-1] |= np.uint64(1 << 63)
+        mods.append(m)
+        bases.append(rng.integers(0, 2**64, k, dtype=np.uint64))
+        exps.append(e)
+    dm = [torch.from_numpy(x).cuda() for x in mods]
+    db = [torch.from_numpy(x).cuda() for x in bases]
+    de = [torch.from_numpy(x).cuda() for x in exps]
+    dr = [torch.zeros(k, dtype=torch.uint64, device="cuda") for _ in range(n)]
+    d = (nbgpu.PowmodDesc * n)()
+    for i in range(n):
+        d[i] = nbgpu.PowmodDesc(dr[i].data_ptr(), db[i].data_ptr(), de[i].data_ptr(), dm[i].data_ptr(), k, le)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        nbgpu.powermod_batch_dev(d, k)
+    torch.cuda.synchronize()
+    times = []
+    l0 = nbgpu.launch_count()
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            nbgpu.powermod_batch_dev(d, k)
+            times.append(time.perf_counter() - t0)
+    launches = nbgpu.launch_count() - l0
+    res = [r.cpu().numpy() for r in dr]
+    # e2e: host buffers
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        host_res = nbgpu.powermod_batch(bases, exps, mods)
+        e2e_t.append(time.perf_counter() - t0)
+    mism = sum(int(not np.array_equal(a, b)) for a, b in zip(res, host_res))
+    # bit-exactness: a seeded sample against integer pow
+    chk = np.random.default_rng(5).choice(n, min(args.check, n), replace=False)
+    for i in chk:
+        want = pow(oracle.to_int(bases[i]), oracle.to_int(exps[i]), oracle.to_int(mods[i]))
+        mism += int(oracle.to_int(res[i]) != want)
+    if mism:
+        raise SystemExit(f"powmod bench: {mism} results differ")
+    # CPU baseline: the oracle's restatement of powermod_limbs on a sample of chains
+    threads = os.cpu_count() or 1
+    cpu = None
+    if args.cpu_seconds > 0:
+        oracle.powmod_barrett(bases[0], exps[0], mods[0])  # plans cached single-threaded
+        oracle.powmod_barrett(bases[1], exps[1], mods[1])
+        t0 = time.perf_counter()
+        one = oracle.powmod_barrett(bases[2], exps[2], mods[2])
+        per = time.perf_counter() - t0
+        ns = int(max(threads, min(n, args.cpu_seconds * threads / max(per, 1e-3))))
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            t0 = time.perf_counter()
+            outs = list(ex.map(lambda i: oracle.powmod_barrett(bases[i % n], exps[i % n], mods[i % n]), range(ns)))
+            dt = time.perf_counter() - t0
+        if any(not np.array_equal(outs[i], res[i % n]) for i in range(ns)) or not np.array_equal(one, res[2]):
+            raise SystemExit("powmod bench: CPU oracle differs from the GPU")
+        cpu = {"value": ns / dt, "unit": "chains/s", "cores": threads, "kind": "port",
+               "sample": f"{ns} chains of the same workload, {threads} threads; CPU restatement of "
+                         "src/algorithms.jl powermod_limbs + src/barrett.jl with fp-NTT products"}
+    med = statistics.median(times)
+    line = {
+        "metric": "Barrett powermod chains/s (256 chains, 16384-bit moduli, 4096-bit exponents), bit-exact",
+        "mode": "powmod", "impl": "ours", "value": n / med, "unit": "chains/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * med, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": POWMOD_WORKLOAD, "chains": n, "k": k, "exponent_bits": 64 * le, "seed": args.seed,
+                   "timing": "wall clock around each synchronous call (setup, all steps, result copy)"},
+        "e2e": {"value": n / statistics.median(e2e_t), "unit": "chains/s",
+                "h2d_bytes_per_step": int(8 * n * (2 * k + le)), "d2h_bytes_per_step": int(8 * n * k)},
+        "gpu_launches": int(launches / max(1, args.steps)),
+        "bitexact": {"checked_vs_pow": int(len(chk)), "gpu_host_vs_device_equal": True, "mismatches": 0},
+        "cpu_baseline": cpu, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -617,6 +716,9 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--shape", default="", help="m,n: a batch of one product shape instead of the mixed workload")
     ap.add_argument("--square", action="store_true", help="with --shape: squares of m-limb operands")
+    ap.add_argument("--powmod", action="store_true", help="Barrett powermod chains (256-limb moduli)")
+    ap.add_argument("--powmod-chains", type=int, default=256)
+    ap.add_argument("--powmod-ebits", type=int, default=4096, help="exponent bits (a multiple of 64)")
     ap.add_argument("--serve", action="store_true", help="serving loop at swept Poisson arrival rates")
     ap.add_argument("--serve-rates", default="1000,5000,20000,50000,200000")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
@@ -634,7 +736,10 @@ def main() -> None:
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        if args.serve:
+        if args.powmod:
+            if rank == 0:
+                run_powmod(args)
+        elif args.serve:
             if rank == 0:
                 run_serve(args)
         elif args.impl == "reference":

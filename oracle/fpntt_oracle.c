@@ -23,6 +23,7 @@
  * the reference schedule.
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -611,17 +612,25 @@ int orc_ntt_params(int64_t bits_a, int64_t bits_b, int *b_out, int64_t *N_out) {
 #define ORC_CACHE 1024
 static struct { int64_t N; int f; orc_plan *pl; } orc_cache[ORC_CACHE];
 static int orc_ncache = 0;
+/* The cache is shared by the threads of the timed CPU baseline: one lock. */
+static pthread_mutex_t orc_cache_mu = PTHREAD_MUTEX_INITIALIZER;
+
 orc_plan *orc_plan_get(int64_t N, int f) {
+    pthread_mutex_lock(&orc_cache_mu);
     for (int i = 0; i < orc_ncache; i++)
-        if (orc_cache[i].N == N && orc_cache[i].f == f) return orc_cache[i].pl;
+        if (orc_cache[i].N == N && orc_cache[i].f == f) {
+            orc_plan *hit = orc_cache[i].pl;
+            pthread_mutex_unlock(&orc_cache_mu);
+            return hit;
+        }
     orc_plan *pl = orc_plan_build(N, f);
-    if (!pl) return NULL;
-    if (orc_ncache < ORC_CACHE) {
+    if (pl && orc_ncache < ORC_CACHE) {
         orc_cache[orc_ncache].N = N;
         orc_cache[orc_ncache].f = f;
         orc_cache[orc_ncache].pl = pl;
         orc_ncache++;
     }
+    pthread_mutex_unlock(&orc_cache_mu);
     return pl;
 }
 
@@ -676,5 +685,185 @@ int orc_sqr_fpntt2(uint64_t *r, const uint64_t *a, int64_t n) {
     orc_ntt_rev(tmp2, plan2);
     orc_unpack2(r, 2 * n, tmp1, tmp2, N, 2 * nca - 1, bch, plan1->ninv, plan1->ninvp, plan2->ninv, plan2->ninvp);
     free(buf);
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Barrett powermod (the workload of the powermod chains): a restatement of
+ * powermod_limbs on its Barrett branch (src/algorithms.jl:17-107) with
+ * barrett_mu!/barrett_reduce! (src/barrett.jl:22-81); every product goes
+ * through the fp NTT above, as the reference's mul!/sqr! do at 256 limbs.
+ * ------------------------------------------------------------------------ */
+
+static int64_t orc_normlen(const uint64_t *a, int64_t n) {
+    while (n > 0 && a[n - 1] == 0) n--;
+    return n;
+}
+
+/* a[0..n) >= b[0..nb), nb <= n (missing limbs zero) */
+static int orc_geq(const uint64_t *a, int64_t n, const uint64_t *b, int64_t nb) {
+    for (int64_t i = n - 1; i >= 0; i--) {
+        uint64_t y = i < nb ? b[i] : 0;
+        if (a[i] != y) return a[i] > y;
+    }
+    return 1;
+}
+
+/* r[0..n) = a[0..n) - b[0..nb) mod 2^(64n) */
+static void orc_subn(uint64_t *r, const uint64_t *a, int64_t n, const uint64_t *b, int64_t nb) {
+    uint64_t br = 0;
+    for (int64_t i = 0; i < n; i++) {
+        uint64_t y = i < nb ? b[i] : 0, x = a[i];
+        uint64_t d = x - y - br;
+        br = (x < y) || (x - y < br);
+        r[i] = d;
+    }
+}
+
+/* r = a * b for normalized lengths (either may be zero) into r[0..m+n) */
+static void orc_mul_any(uint64_t *r, const uint64_t *a, int64_t m, const uint64_t *b, int64_t n) {
+    int64_t la = orc_normlen(a, m), lb = orc_normlen(b, n);
+    memset(r, 0, sizeof(uint64_t) * (size_t)(m + n));
+    if (!la || !lb) return;
+    if (a == b && la == lb) orc_sqr_fpntt2(r, a, la);
+    else orc_mul_fpntt2(r, a, la, b, lb);
+}
+
+/* mu[0..k+2) = floor(2^(128k) / m): schoolbook division by one-limb estimates
+ * corrected downward (the remainder is kept exact), divrem!'s role in
+ * barrett_mu!.  Returns mu's normalized length. */
+int64_t orc_barrett_mu(const uint64_t *m, int64_t k, uint64_t *mu) {
+    typedef unsigned __int128 u128;
+    uint64_t *rem = (uint64_t *)calloc((size_t)(k + 1), sizeof(uint64_t));
+    uint64_t *t = (uint64_t *)calloc((size_t)(k + 1), sizeof(uint64_t));
+    memset(mu, 0, sizeof(uint64_t) * (size_t)(k + 2));
+    /* numerator digits from the top: 1 followed by 2k zero limbs */
+    for (int64_t j = 2 * k; j >= 0; j--) {
+        /* rem = rem * 2^64 + digit */
+        memmove(rem + 1, rem, sizeof(uint64_t) * (size_t)k);
+        rem[0] = j == 2 * k ? 1 : 0;
+        /* q = floor(rem / m) < 2^64; estimate from the top two limbs of rem and the top limb of m */
+        uint64_t q = 0;
+        if (orc_geq(rem, k + 1, m, k)) {
+            u128 top = ((u128)rem[k] << 64) | rem[k - 1];
+            u128 est = top / ((u128)m[k - 1]);
+            q = est >> 64 ? ~(uint64_t)0 : (uint64_t)est;
+            for (;;) { /* t = q*m; lower q until t <= rem */
+                uint64_t c = 0;
+                for (int64_t i = 0; i < k; i++) {
+                    u128 p = (u128)q * m[i] + c;
+                    t[i] = (uint64_t)p;
+                    c = (uint64_t)(p >> 64);
+                }
+                t[k] = c;
+                if (orc_geq(rem, k + 1, t, k + 1)) break;
+                /* overshoot: step q down by about (t - rem) / m */
+                uint64_t *d = (uint64_t *)calloc((size_t)(k + 1), sizeof(uint64_t));
+                orc_subn(d, t, k + 1, rem, k + 1);
+                u128 dt = ((u128)d[k] << 64) | d[k - 1];
+                u128 dec = dt / ((u128)m[k - 1] + 1) + 1;
+                free(d);
+                q = dec >= q ? 0 : q - (uint64_t)dec;
+            }
+            orc_subn(rem, rem, k + 1, t, k + 1);
+            while (orc_geq(rem, k + 1, m, k)) { /* q too small */
+                orc_subn(rem, rem, k + 1, m, k);
+                q++;
+            }
+        }
+        if (j < k + 2) mu[j] = q;
+    }
+    free(rem);
+    free(t);
+    return orc_normlen(mu, k + 2);
+}
+
+/* barrett_reduce! (barrett.jl:44-81): r[0..k) = T mod m, T = t[0..2k) (t[2k] = 0). */
+static void orc_barrett_reduce(uint64_t *r, const uint64_t *t, const uint64_t *m, int64_t k, const uint64_t *mu,
+                               int64_t lmu, uint64_t *scratch) {
+    const int64_t kp1 = k + 1;
+    uint64_t *q2 = scratch, *r2 = scratch + 2 * k + 3;
+    int64_t l1 = orc_normlen(t + k - 1, kp1), lq3 = 0;
+    if (l1 > 0) {
+        orc_mul_any(q2, t + k - 1, l1, mu, lmu);
+        lq3 = orc_normlen(q2 + kp1, l1 + lmu - kp1);
+    }
+    if (lq3 == 0) {
+        memcpy(scratch, t, sizeof(uint64_t) * (size_t)kp1);
+    } else {
+        orc_mul_any(r2, m, k, q2 + kp1, lq3);
+        orc_subn(scratch, t, kp1, r2, kp1);
+    }
+    int64_t lr = orc_normlen(scratch, kp1);
+    while (orc_geq(scratch, kp1, m, k)) {
+        orc_subn(scratch, scratch, kp1, m, k);
+        lr = orc_normlen(scratch, lr);
+    }
+    memcpy(r, scratch, sizeof(uint64_t) * (size_t)lr);
+    memset(r + lr, 0, sizeof(uint64_t) * (size_t)(k - lr));
+}
+
+static int orc_expbit(const uint64_t *e, int64_t i) { return (int)((e[i >> 6] >> (i & 63)) & 1); }
+
+/* powermod_limbs, Barrett branch: r[0..k) = b^e mod m.  b[0..lb) with lb <= k
+ * (reduced mod m first), e[0..le) nonzero, m[k-1] != 0, m > 1. */
+int orc_powmod_barrett(uint64_t *r, const uint64_t *b, int64_t lb, const uint64_t *e, int64_t le, const uint64_t *m,
+                       int64_t k) {
+    int64_t nbits = 0;
+    for (int64_t i = le - 1; i >= 0 && !nbits; i--)
+        if (e[i]) nbits = 64 * i + 64 - (int64_t)__builtin_clzll(e[i]);
+    if (!nbits || lb > k || !m[k - 1]) return -1;
+    const int w = nbits <= 8 ? 1 : nbits <= 24 ? 2 : nbits <= 80 ? 3 : nbits <= 240 ? 4 : 5;
+    const int tsize = 1 << (w - 1);
+    uint64_t *mu = (uint64_t *)calloc((size_t)(k + 2), 8);
+    uint64_t *scratch = (uint64_t *)calloc((size_t)(4 * k + 6), 8);
+    uint64_t *prod = (uint64_t *)calloc((size_t)(2 * k + 1), 8);
+    uint64_t *table = (uint64_t *)calloc((size_t)(tsize * k), 8);
+    uint64_t *acc = (uint64_t *)calloc((size_t)k, 8);
+    uint64_t *bsq = (uint64_t *)calloc((size_t)k, 8);
+    const int64_t lmu = orc_barrett_mu(m, k, mu);
+#define MULRED(dst, x, y)                                  \
+    do {                                                   \
+        orc_mul_any(prod, (x), k, (y), k);                 \
+        prod[2 * k] = 0;                                   \
+        orc_barrett_reduce((dst), prod, m, k, mu, lmu, scratch); \
+    } while (0)
+    /* slot 0 = b mod m (the reference reduces b before powermod_limbs) */
+    memset(prod, 0, sizeof(uint64_t) * (size_t)(2 * k + 1));
+    memcpy(prod, b, sizeof(uint64_t) * (size_t)lb);
+    orc_barrett_reduce(table, prod, m, k, mu, lmu, scratch);
+    if (tsize > 1) {
+        MULRED(bsq, table, table);
+        for (int j = 1; j < tsize; j++) MULRED(table + j * k, table + (j - 1) * k, bsq);
+    }
+    int first = 1;
+    int64_t i = nbits - 1;
+    while (i >= 0) {
+        if (!orc_expbit(e, i)) {
+            if (!first) MULRED(acc, acc, acc);
+            i--;
+            continue;
+        }
+        int64_t l = w < i + 1 ? w : i + 1;
+        while (!orc_expbit(e, i - l + 1)) l--;
+        int val = 0;
+        for (int64_t j = 0; j < l; j++) val = (val << 1) | orc_expbit(e, i - j);
+        if (first) {
+            memcpy(acc, table + (val >> 1) * k, sizeof(uint64_t) * (size_t)k);
+            first = 0;
+        } else {
+            for (int64_t j = 0; j < l; j++) MULRED(acc, acc, acc);
+            MULRED(acc, acc, table + (val >> 1) * k);
+        }
+        i -= l;
+    }
+#undef MULRED
+    memcpy(r, acc, sizeof(uint64_t) * (size_t)k);
+    free(mu);
+    free(scratch);
+    free(prod);
+    free(table);
+    free(acc);
+    free(bsq);
     return 0;
 }

@@ -72,6 +72,8 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         "orc_ntt_params": (c.c_int, [c.c_int64, c.c_int64, c.POINTER(c.c_int), c.POINTER(c.c_int64)]),
         "orc_mul_fpntt2": (c.c_int, [_u64p, _u64p, c.c_int64, _u64p, c.c_int64]),
         "orc_sqr_fpntt2": (c.c_int, [_u64p, _u64p, c.c_int64]),
+        "orc_barrett_mu": (c.c_int64, [_u64p, c.c_int64, _u64p]),
+        "orc_powmod_barrett": (c.c_int, [_u64p, _u64p, c.c_int64, _u64p, c.c_int64, _u64p, c.c_int64]),
         "orc_op_count": (c.c_uint64, []),
         "orc_op_count_reset": (None, []),
     }
@@ -258,6 +260,27 @@ def gmp_sqr(a: np.ndarray) -> np.ndarray:
     a = np.ascontiguousarray(a, dtype=np.uint64)
     r = np.zeros(2 * len(a), dtype=np.uint64)
     gmp().__gmpn_sqr(_p(r, _u64p), _p(a, _u64p), len(a))
+    return r
+
+
+def barrett_mu(m: np.ndarray) -> np.ndarray:
+    """barrett_mu! (src/barrett.jl:22-31): floor(2^(128k) / m), k + 2 limbs."""
+    m = np.ascontiguousarray(m, dtype=np.uint64)
+    mu = np.zeros(m.size + 2, dtype=np.uint64)
+    lib().orc_barrett_mu(_p(m, _u64p), m.size, _p(mu, _u64p))
+    return mu
+
+
+def powmod_barrett(b: np.ndarray, e: np.ndarray, m: np.ndarray) -> np.ndarray:
+    """powermod_limbs on its Barrett branch (src/algorithms.jl:17-107):
+    b^e mod m, k = len(m) limbs, every product through the fp NTT."""
+    b = np.ascontiguousarray(b, dtype=np.uint64)
+    e = np.ascontiguousarray(e, dtype=np.uint64)
+    m = np.ascontiguousarray(m, dtype=np.uint64)
+    r = np.zeros(m.size, dtype=np.uint64)
+    rc = lib().orc_powmod_barrett(_p(r, _u64p), _p(b, _u64p), b.size, _p(e, _u64p), e.size, _p(m, _u64p), m.size)
+    if rc:
+        raise ValueError("powmod_barrett: bad arguments")
     return r
 
 

@@ -78,3 +78,18 @@ def test_schedule_window_widths():
         assert T == 1 << (w - 1), bits
     with pytest.raises(Exception):
         powmod_schedule(np.zeros(2, dtype=np.uint64))
+
+
+@pytest.mark.parametrize("k", [1, 2, 5, 64])
+def test_oracle_mu_and_powmod(k):
+    """The oracle's restatement (the CPU baseline of the chains) against integers."""
+    rng = np.random.default_rng(40 + k)
+    for i in range(3):
+        m = rand_limbs(rng, k)
+        m[0] = (int(m[0]) | 1) if i % 2 else (int(m[0]) & ~1)
+        if k == 1:
+            m[0] = max(int(m[0]), 2)
+        assert _int(O.barrett_mu(m)) == B ** (2 * k) // _int(m)
+        b = rand_limbs(rng, k)
+        e = rand_limbs(rng, 2 if k > 5 else 5)
+        assert _int(O.powmod_barrett(b, e, m)) == pow(_int(b), _int(e), _int(m))

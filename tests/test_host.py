@@ -287,3 +287,15 @@ def test_autotune_candidates_emulate_cleanly():
                 _emulate_plan(N, lay)
     finally:
         nbgpu.set_tuning(old)
+
+
+def test_odd_multiplier_landings():
+    """Balanced sizes that land on each odd transform-length multiplier (the
+    single-product configuration's list), by the oracle and the library."""
+    import nbgpu
+
+    for n, N in ((4096, 3 * 2**12), (6200, 5 * 2**12), (9032, 7 * 2**12), (5512, 9 * 2**11),
+                 (110336, 3 * 2**17), (94592, 5 * 2**16), (68992, 7 * 2**15), (84096, 9 * 2**15),
+                 (1439744, 315 * 2**14), (10928128, 315 * 2**17)):
+        assert O.ntt_params(64 * n, 64 * n)[1] == N
+        assert nbgpu.ntt_params(64 * n, 64 * n)[1] == N

@@ -703,6 +703,44 @@ def run_powmod(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_route(args) -> None:
+    """Per-call time of unbalanced products below the reference's NTT admission
+    (smaller operand n < 64: its chunked Karatsuba path) on the GPU (nbg_mul,
+    host buffers, copies included) against GMP's mpn_mul on one host core, to
+    place the routing threshold.  One JSON line with the grid of timings."""
+    import nbgpu
+    import oracle
+
+    nbgpu._check(nbgpu.lib().nbg_init(0))
+    rng = np.random.Generator(np.random.PCG64(args.seed))
+    rows = []
+    for n in (8, 29, 48, 63):
+        for m in (1000, 10000, 100000, 1000000):
+            a = rng.integers(0, 2**64, m, dtype=np.uint64)
+            b = rng.integers(0, 2**64, n, dtype=np.uint64)
+            a[-1] |= np.uint64(1)
+            b[-1] |= np.uint64(1)
+            want = oracle.gmp_mul(a, b)
+            got = nbgpu.mul(a, b)
+            if not np.array_equal(got, want):
+                raise SystemExit(f"route bench: {m}x{n} differs from GMP")
+            reps = max(3, int(2e6 / (m * n ** 0.585)))
+            ts = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                nbgpu.mul(a, b)
+                ts.append(time.perf_counter() - t0)
+            tg = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                oracle.gmp_mul(a, b)
+                tg.append(time.perf_counter() - t0)
+            rows.append({"m": m, "n": n, "gpu_us": 1e6 * statistics.median(ts), "gmp_us": 1e6 * statistics.median(tg),
+                         "work": m * n ** 0.585})
+    print(json.dumps({"mode": "route", "metric": "per-call us, unbalanced products below NTT admission",
+                      "rows": rows, "data": "synthetic", "n_gpus": 1}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -717,6 +755,7 @@ def main() -> None:
     ap.add_argument("--shape", default="", help="m,n: a batch of one product shape instead of the mixed workload")
     ap.add_argument("--square", action="store_true", help="with --shape: squares of m-limb operands")
     ap.add_argument("--powmod", action="store_true", help="Barrett powermod chains (256-limb moduli)")
+    ap.add_argument("--route", action="store_true", help="per-call timings of products below NTT admission")
     ap.add_argument("--powmod-chains", type=int, default=256)
     ap.add_argument("--powmod-ebits", type=int, default=4096, help="exponent bits (a multiple of 64)")
     ap.add_argument("--serve", action="store_true", help="serving loop at swept Poisson arrival rates")
@@ -736,7 +775,10 @@ def main() -> None:
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        if args.powmod:
+        if args.route:
+            if rank == 0:
+                run_route(args)
+        elif args.powmod:
             if rank == 0:
                 run_powmod(args)
         elif args.serve:

@@ -39,6 +39,14 @@ int nbg_mul(uint64_t *r, const uint64_t *a, int64_t m, const uint64_t *b, int64_
  * branch of sqr! (src/mul.jl:141-147, :134). */
 int nbg_sqr(uint64_t *r, const uint64_t *a, int64_t n);
 
+/* r[0..k) = a[0..la) * b[0..lb) mod 2^(64k) (a^2 for nbg_sqrlo), la, lb, k >= 1;
+ * r holds exactly k limbs and must not alias an input.  Replaces the
+ * full-product branches of mullo!/sqrlo! (src/mul.jl:316-319, :361-364),
+ * which keep the low k limbs of mul!/sqr!, and extends them below the
+ * reference's MULLO_FULL_THRESHOLD / SQRLO_FULL_THRESHOLD (src/mul.jl:183-184). */
+int nbg_mullo(uint64_t *r, const uint64_t *a, int64_t la, const uint64_t *b, int64_t lb, int64_t k);
+int nbg_sqrlo(uint64_t *r, const uint64_t *a, int64_t la, int64_t k);
+
 /* ---- products, device buffers (asynchronous on `stream`, a cudaStream_t; ----
  * ---- NULL is the legacy default stream)                                  - */
 

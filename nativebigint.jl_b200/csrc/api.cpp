@@ -466,6 +466,35 @@ int nbg_sqr(uint64_t* r, const uint64_t* a, int64_t n) {
     return host_batch(&d, 1);
 }
 
+// Low halves: operand limbs at or above k cannot reach the low k limbs, so
+// the operands are cut to k limbs, the full product runs on the GPU, and its
+// low k limbs are kept (the reference's full-product branches of mullo! and
+// sqrlo!, src/mul.jl:316-319 and :361-364, at every size).
+static int low_product(uint64_t* r, const uint64_t* a, int64_t la, const uint64_t* b, int64_t lb, int64_t k) {
+    if (!r || !a || la < 1 || k < 1 || (b && lb < 1)) return fail(NBG_EINVAL, "bad argument");
+    la = std::min(la, k);
+    lb = b ? std::min(lb, k) : la;
+    std::vector<uint64_t> full((size_t)(la + lb));
+    nbg_desc d{full.data(), a, b, la, lb, 0, 0};
+    int rc = host_batch(&d, 1);
+    if (rc) return rc;
+    const int64_t keep = std::min(k, la + lb);
+    memcpy(r, full.data(), sizeof(uint64_t) * (size_t)keep);
+    if (keep < k) memset(r + keep, 0, sizeof(uint64_t) * (size_t)(k - keep));
+    return NBG_OK;
+}
+
+int nbg_mullo(uint64_t* r, const uint64_t* a, int64_t la, const uint64_t* b, int64_t lb, int64_t k) {
+    if (!b) return fail(NBG_EINVAL, "null pointer");
+    API_LOCK();
+    return low_product(r, a, la, b, lb, k);
+}
+
+int nbg_sqrlo(uint64_t* r, const uint64_t* a, int64_t la, int64_t k) {
+    API_LOCK();
+    return low_product(r, a, la, nullptr, 0, k);
+}
+
 int nbg_mul_dev(uint64_t* r, const uint64_t* a, int64_t m, const uint64_t* b, int64_t n, void* stream) {
     if (!b) return fail(NBG_EINVAL, "null pointer");
     API_LOCK();

@@ -54,6 +54,40 @@ function gpu_sqr_fpntt2!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, n::
     return nothing
 end
 
+# r[ro+1 .. ro+k] = low k limbs of a*b (the full-product branch of mullo!,
+# src/mul.jl:316-319) and of a^2 (sqrlo!, :361-364)
+function gpu_mullo!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, la::Int,
+                    b::Memory{Limb}, bo::Int, lb::Int, k::Int)
+    @boundscheck (ro + k <= length(r) && ao + la <= length(a) && bo + lb <= length(b)) || throw(BoundsError())
+    GC.@preserve r a b begin
+        rc = ccall((:nbg_mullo, LIB), Cint, (Ptr{Limb}, Ptr{Limb}, Int64, Ptr{Limb}, Int64, Int64),
+                   pointer(r, ro + 1), pointer(a, ao + 1), la, pointer(b, bo + 1), lb, k)
+    end
+    check(rc)
+    return nothing
+end
+
+function gpu_sqrlo!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, la::Int, k::Int)
+    @boundscheck (ro + k <= length(r) && ao + la <= length(a)) || throw(BoundsError())
+    GC.@preserve r a begin
+        rc = ccall((:nbg_sqrlo, LIB), Cint, (Ptr{Limb}, Ptr{Limb}, Int64, Int64),
+                   pointer(r, ro + 1), pointer(a, ao + 1), la, k)
+    end
+    check(rc)
+    return nothing
+end
+
+# Where an m x n product (m >= n) goes once the GPU is installed: the
+# reference's CPU kernels below its NTT admission (src/mul.jl:12-26, :383-390)
+# unless the product is large enough to pay for a GPU call.  The chunked
+# Karatsuba path for n < MUL_FPNTT_MIN costs about m*n^0.585 limb operations
+# there, so long unbalanced products with a small operand move to the GPU.
+# Measured on B200 (bench.py --route): one host-buffer GPU call costs about
+# 75 us and overtakes GMP's mpn_mul near m*n^0.585 = 1e5 (m = 1e4, n = 29:
+# 101 us vs 133 us; m = 1e6, n = 63: 1.35 ms vs 19.6 ms).
+const GPU_CHUNKED_MIN_WORK = 1.0e5   # m * n^0.585 above which a call pays off
+route_to_gpu(m::Int, n::Int) = (n >= 64 && m + n >= 304) || m * Float64(n)^0.585 >= GPU_CHUNKED_MIN_WORK
+
 # Batched products: descs as in include/nbgpu.h (nbg_desc); b == C_NULL squares a.
 struct NbgDesc
     r::Ptr{Limb}

@@ -39,6 +39,7 @@ EXPORTS = [
     "nbg_server_create", "nbg_submit", "nbg_submit_dev", "nbg_poll", "nbg_wait", "nbg_release",
     "nbg_server_stats", "nbg_server_destroy",
     "nbg_powermod_batch", "nbg_powermod_batch_dev", "nbg_barrett_mu", "nbg_powmod_schedule",
+    "nbg_mullo", "nbg_sqrlo",
 ]
 
 
@@ -106,6 +107,8 @@ def lib() -> ctypes.CDLL:
             "nbg_server_destroy": [vp],
             "nbg_load_tuning": [c.c_char_p],
             "nbg_powermod_batch": [vp, i64, i64],
+            "nbg_mullo": [vp, vp, i64, vp, i64, i64],
+            "nbg_sqrlo": [vp, vp, i64, i64],
             "nbg_powermod_batch_dev": [vp, i64, i64, vp],
         }
         for name, args in sig.items():
@@ -195,6 +198,22 @@ def sqr(a) -> np.ndarray:
     a = _u64(a)
     r = np.empty(2 * a.size, dtype=np.uint64)
     sqr_(r, 0, a, 0, a.size)
+    return r
+
+
+def mullo(a, b, k: int) -> np.ndarray:
+    """Low k limbs of a*b (mullo!'s full-product branch, src/mul.jl:316-319)."""
+    a, b = _u64(a), _u64(b)
+    r = np.empty(k, dtype=np.uint64)
+    _check(lib().nbg_mullo(_ptr(r), _ptr(a), a.size, _ptr(b), b.size, k))
+    return r
+
+
+def sqrlo(a, k: int) -> np.ndarray:
+    """Low k limbs of a^2 (sqrlo!'s full-product branch, src/mul.jl:361-364)."""
+    a = _u64(a)
+    r = np.empty(k, dtype=np.uint64)
+    _check(lib().nbg_sqrlo(_ptr(r), _ptr(a), a.size, k))
     return r
 
 

@@ -202,6 +202,19 @@ int64_t nbg_barrett_mu(const uint64_t *m, int64_t k, uint64_t *mu);
  * Host only. */
 int64_t nbg_powmod_schedule(const uint64_t *e, int64_t le, uint8_t *ops, int64_t cap, int32_t *tsize);
 
+/* ---- sums of products (HGCD callers) --------------------------------------- */
+
+/* M <- M * M1 for 2x2 matrices of nonnegative integers, device buffers, entry
+ * order (m00, m01, m10, m11).  M's entries hold n limbs (zero-padded) and
+ * have room for n + n1 + 1, which they receive; M1's hold n1.  The eight
+ * products run as one GPU batch (zero entries drop out), the four sums on the
+ * GPU.  Replaces hgcd_matrix_mul! (src/gcd.jl:371-389).  Returns when done. */
+int nbg_matrix22_mul_dev(uint64_t *const *m, int64_t n, const uint64_t *const *m1, int64_t n1, void *stream);
+/* r[0..rn) = a*x + b*y, nonnegative, device buffers, rn >= max(la+lx, lb+ly)+1
+ * (cof_mul2!, src/gcd.jl:571-598).  Returns when done. */
+int nbg_mul2add_dev(uint64_t *r, int64_t rn, const uint64_t *a, int64_t la, const uint64_t *x, int64_t lx,
+                    const uint64_t *b, int64_t lb, const uint64_t *y, int64_t ly, void *stream);
+
 /* ---- admission (host-side restatement of the reference's sizing) -------- */
 
 /* fp_ntt_params (src/fpntt.jl:964-977): chunk width b and transform length N. */

@@ -25,7 +25,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompile
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wextra",
              "-Wno-unused-parameter", f"-I{CUDA}/include"]
 
-CU_SOURCES = ["kernels.cu", "noalloc.cu", "powmod_kernels.cu"]
+CU_SOURCES = ["kernels.cu", "noalloc.cu", "powmod_kernels.cu", "linalg.cu"]
 CXX_SOURCES = ["engine.cpp", "api.cpp", "serve.cpp", "powmod.cpp"]
 
 

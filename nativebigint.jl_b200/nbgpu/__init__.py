@@ -39,7 +39,7 @@ EXPORTS = [
     "nbg_server_create", "nbg_submit", "nbg_submit_dev", "nbg_poll", "nbg_wait", "nbg_release",
     "nbg_server_stats", "nbg_server_destroy",
     "nbg_powermod_batch", "nbg_powermod_batch_dev", "nbg_barrett_mu", "nbg_powmod_schedule",
-    "nbg_mullo", "nbg_sqrlo",
+    "nbg_mullo", "nbg_sqrlo", "nbg_matrix22_mul_dev", "nbg_mul2add_dev",
 ]
 
 
@@ -108,6 +108,8 @@ def lib() -> ctypes.CDLL:
             "nbg_load_tuning": [c.c_char_p],
             "nbg_powermod_batch": [vp, i64, i64],
             "nbg_mullo": [vp, vp, i64, vp, i64, i64],
+            "nbg_matrix22_mul_dev": [vp, i64, vp, i64, vp],
+            "nbg_mul2add_dev": [vp, i64, vp, i64, vp, i64, vp, i64, vp, i64, vp],
             "nbg_sqrlo": [vp, vp, i64, i64],
             "nbg_powermod_batch_dev": [vp, i64, i64, vp],
         }
@@ -215,6 +217,20 @@ def sqrlo(a, k: int) -> np.ndarray:
     r = np.empty(k, dtype=np.uint64)
     _check(lib().nbg_sqrlo(_ptr(r), _ptr(a), a.size, k))
     return r
+
+
+def matrix22_mul_dev(m, n: int, m1, n1: int, stream=None) -> None:
+    """M <- M*M1 in place (hgcd_matrix_mul!): m, m1 are 4 device buffers each
+    (m00, m01, m10, m11); m's entries need n + n1 + 1 limbs of room."""
+    pm = (ctypes.c_void_p * 4)(*[_dptr(x) for x in m])
+    pm1 = (ctypes.c_void_p * 4)(*[_dptr(x) for x in m1])
+    _check(lib().nbg_matrix22_mul_dev(pm, n, pm1, n1, _stream(stream)))
+
+
+def mul2add_dev(r, rn: int, a, la: int, x, lx: int, b, lb: int, y, ly: int, stream=None) -> None:
+    """r = a*x + b*y on device buffers (cof_mul2!)."""
+    _check(lib().nbg_mul2add_dev(_dptr(r), rn, _dptr(a), la, _dptr(x), lx, _dptr(b), lb, _dptr(y), ly,
+                                 _stream(stream)))
 
 
 def mul_batch(pairs) -> list[np.ndarray]:

@@ -215,6 +215,13 @@ int nbg_matrix22_mul_dev(uint64_t *const *m, int64_t n, const uint64_t *const *m
 int nbg_mul2add_dev(uint64_t *r, int64_t rn, const uint64_t *a, int64_t la, const uint64_t *x, int64_t lx,
                     const uint64_t *b, int64_t lb, const uint64_t *y, int64_t ly, void *stream);
 
+/* Value of the little-endian base-bb chunks chunks[0..n) (each < bb, 2 <= bb)
+ * as binary limbs: out[0..*out_len) normalized, cap >= n.  The reference's
+ * subquadratic radix_combine (src/nbig.jl:410-417) with its power table by
+ * repeated squaring (:396-399); every level's products run as one GPU batch.
+ * Host buffers. */
+int nbg_radix_combine(uint64_t *out, int64_t cap, const uint64_t *chunks, int64_t n, uint64_t bb, int64_t *out_len);
+
 /* ---- admission (host-side restatement of the reference's sizing) -------- */
 
 /* fp_ntt_params (src/fpntt.jl:964-977): chunk width b and transform length N. */

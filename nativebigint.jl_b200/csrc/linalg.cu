@@ -165,6 +165,28 @@ __global__ void __launch_bounds__(256) k_magbits(const uint64_t* const* __restri
     }
 }
 
+// Radix combine, first level: node i = value of the base-bb chunks
+// c[32i .. 32i+31] (chunks past n read as zero) by Horner's rule, one thread
+// per node, into out[32i .. 32i+31] (the value is below bb^32 < 2^2048).
+__global__ void __launch_bounds__(128) k_horner32(const uint64_t* __restrict__ c, int64_t n, uint64_t bb,
+                                                  uint64_t* __restrict__ out, int64_t nodes) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    uint64_t* v = out + 32 * i;
+    for (int w = 0; w < 32; w++) v[w] = 0;
+    int len = 0;  // limbs of v in use
+    for (int j = 31; j >= 0; j--) {
+        const int64_t idx = 32 * i + j;
+        uint64_t carry = idx < n ? c[idx] : 0;  // v = v * bb + c_j
+        for (int w = 0; w < len; w++) {
+            const unsigned __int128 t = (unsigned __int128)v[w] * bb + carry;
+            v[w] = (uint64_t)t;
+            carry = (uint64_t)(t >> 64);
+        }
+        if (carry && len < 32) v[len++] = carry;
+    }
+}
+
 }  // namespace nbg
 
 using namespace nbg;
@@ -177,10 +199,12 @@ namespace {
         if (e_ != cudaSuccess) return fail(NBG_ECUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
     } while (0)
 
-// out[k] = Σ over terms t with owner[t] == k of a_t * b_t (device buffers,
-// nonnegative), out[k] holding outlen[k] limbs.  At most two terms per output.
+// out[k] = Σ over terms t with owner[t] == k of a_t * b_t, plus addend[k]
+// when given (device buffers, nonnegative), out[k] holding outlen[k] limbs.
+// At most two summands per output.
 int sum_products(const std::vector<nbg_desc>& terms, const std::vector<int>& owner,
-                 const std::vector<uint64_t*>& out, const std::vector<int64_t>& outlen, cudaStream_t st) {
+                 const std::vector<uint64_t*>& out, const std::vector<int64_t>& outlen, cudaStream_t st,
+                 const std::vector<std::pair<const uint64_t*, int64_t>>* addend = nullptr) {
     const int nt = (int)terms.size(), no = (int)out.size();
     // magnitude bits of every operand, read on the device
     std::vector<const uint64_t*> bufs(2 * (size_t)nt);
@@ -207,13 +231,15 @@ int sum_products(const std::vector<nbg_desc>& terms, const std::vector<int>& own
         cudaStream_t s;
         ~Free() { cudaFreeAsync(p, s); }
     } guard{d, st};
-    LA_TRY(cudaMemcpyAsync(d + off_bufs, bufs.data(), 8 * bufs.size(), cudaMemcpyHostToDevice, st));
-    LA_TRY(cudaMemcpyAsync(d + off_lens, lens.data(), 8 * lens.size(), cudaMemcpyHostToDevice, st));
-    k_magbits<<<(unsigned)(2 * nt), 256, 0, st>>>((const uint64_t* const*)(d + off_bufs),
-                                                   (const int64_t*)(d + off_lens), (int64_t*)(d + off_bits));
-    LA_TRY(cudaGetLastError());
-    LA_TRY(cudaMemcpyAsync(bits.data(), d + off_bits, 8 * bits.size(), cudaMemcpyDeviceToHost, st));
-    LA_TRY(cudaStreamSynchronize(st));
+    if (nt > 0) {
+        LA_TRY(cudaMemcpyAsync(d + off_bufs, bufs.data(), 8 * bufs.size(), cudaMemcpyHostToDevice, st));
+        LA_TRY(cudaMemcpyAsync(d + off_lens, lens.data(), 8 * lens.size(), cudaMemcpyHostToDevice, st));
+        k_magbits<<<(unsigned)(2 * nt), 256, 0, st>>>((const uint64_t* const*)(d + off_bufs),
+                                                       (const int64_t*)(d + off_lens), (int64_t*)(d + off_bits));
+        LA_TRY(cudaGetLastError());
+        LA_TRY(cudaMemcpyAsync(bits.data(), d + off_bits, 8 * bits.size(), cudaMemcpyDeviceToHost, st));
+        LA_TRY(cudaStreamSynchronize(st));
+    }
     // nonzero products into the scratch; zero ones drop out of their sums
     std::vector<nbg_desc> live;
     std::vector<const uint64_t*> prod_of((size_t)nt, nullptr);
@@ -254,6 +280,16 @@ int sum_products(const std::vector<nbg_desc>& terms, const std::vector<int>& own
             } else {
                 J.y = prod_of[(size_t)t];
                 J.ny = prod_len[(size_t)t];
+            }
+        }
+        if (addend && (*addend)[(size_t)k].first) {
+            const auto& ad = (*addend)[(size_t)k];
+            if (!J.x) {
+                J.x = ad.first;
+                J.nx = ad.second;
+            } else {
+                J.y = ad.first;
+                J.ny = ad.second;
             }
         }
         J.ntl = (J.rn + SUM_TL - 1) / SUM_TL;
@@ -308,3 +344,116 @@ int nbg_mul2add_dev(uint64_t* r, int64_t rn, const uint64_t* a, int64_t la, cons
 }
 
 }  // extern "C"
+
+namespace {
+
+// bb^32 on the host (32 limbs), the first entry of the power table.
+void pow32(uint64_t bb, uint64_t* p) {
+    memset(p, 0, 32 * sizeof(uint64_t));
+    p[0] = 1;
+    for (int k = 0; k < 32; k++) {
+        uint64_t carry = 0;
+        for (int w = 0; w < 32; w++) {
+            const unsigned __int128 t = (unsigned __int128)p[w] * bb + carry;
+            p[w] = (uint64_t)t;
+            carry = (uint64_t)(t >> 64);
+        }
+    }
+}
+
+// Value of the little-endian base-bb chunks c[0..n) (device) into the device
+// buffer *res (*res_limbs limbs, zero-padded): radix_combine of the reference
+// (src/nbig.jl:410-417) level by level.  Level 5 (32 chunks per node) is one
+// Horner kernel; every higher level is one batch of products high * bb^(2^(l-1))
+// plus the low halves, the power table built by repeated GPU squaring as the
+// reference's radix_chunks_dc builds it (src/nbig.jl:396-399).
+int radix_combine_run(const uint64_t* d_c, int64_t n, uint64_t bb, std::vector<void*>& keep, uint64_t** res,
+                      int64_t* res_limbs, cudaStream_t st) {
+    int64_t M = 1;
+    while (M < (n + 31) / 32) M <<= 1;
+    const int64_t total = 32 * M;
+    uint64_t *A = nullptr, *Bf = nullptr, *P = nullptr;
+    LA_TRY(cudaMalloc((void**)&A, 8 * (size_t)total));
+    keep.push_back(A);
+    LA_TRY(cudaMalloc((void**)&Bf, 8 * (size_t)total));
+    keep.push_back(Bf);
+    LA_TRY(cudaMemsetAsync(A, 0, 8 * (size_t)total, st));
+    const int64_t nodes5 = (n + 31) / 32;
+    k_horner32<<<(unsigned)((nodes5 + 127) / 128), 128, 0, st>>>(d_c, n, bb, A, nodes5);
+    LA_TRY(cudaGetLastError());
+    g_launches++;
+    // P = bb^32, squared up the levels
+    int64_t plen = 32;
+    LA_TRY(cudaMalloc((void**)&P, 8 * 32));
+    keep.push_back(P);
+    {
+        uint64_t h[32];
+        pow32(bb, h);
+        LA_TRY(cudaMemcpyAsync(P, h, sizeof h, cudaMemcpyHostToDevice, st));
+        LA_TRY(cudaStreamSynchronize(st));
+    }
+    uint64_t *in = A, *out = Bf;
+    for (int64_t s = 64; s <= total; s *= 2) {  // node size of the level being formed
+        const int64_t half = s / 2, count = total / s;
+        std::vector<nbg_desc> terms((size_t)count);
+        std::vector<int> owner((size_t)count);
+        std::vector<uint64_t*> outs((size_t)count);
+        std::vector<int64_t> outlen((size_t)count, s);
+        std::vector<std::pair<const uint64_t*, int64_t>> add((size_t)count);
+        for (int64_t i = 0; i < count; i++) {
+            terms[(size_t)i] = nbg_desc{nullptr, in + (2 * i + 1) * half, P, half, plen, 0, 0};
+            owner[(size_t)i] = (int)i;
+            outs[(size_t)i] = out + i * s;
+            add[(size_t)i] = {in + 2 * i * half, half};
+        }
+        int rc = sum_products(terms, owner, outs, outlen, st, &add);
+        if (rc) return rc;
+        std::swap(in, out);
+        if (2 * s <= total) {  // next power: P^2
+            uint64_t* P2 = nullptr;
+            LA_TRY(cudaMalloc((void**)&P2, 8 * (size_t)(2 * plen)));
+            keep.push_back(P2);
+            rc = nbg_sqr_dev(P2, P, plen, st);
+            if (rc) return rc;
+            P = P2;
+            plen *= 2;
+        }
+    }
+    *res = in;
+    *res_limbs = total;
+    return NBG_OK;
+}
+
+}  // namespace
+
+extern "C" int nbg_radix_combine(uint64_t* out, int64_t cap, const uint64_t* chunks, int64_t n, uint64_t bb,
+                                 int64_t* out_len) {
+    if (!out || !chunks || !out_len || n < 1 || bb < 2 || cap < n) return fail(NBG_EINVAL, "bad argument");
+    for (int64_t i = 0; i < n; i++)
+        if (chunks[i] >= bb) return fail(NBG_EINVAL, "chunk %lld is not below the base", (long long)i);
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    int rc = g_eng.ensure();
+    if (rc) return rc;
+    cudaStream_t st = g_eng.stream;
+    std::vector<void*> keep;
+    struct Free {
+        std::vector<void*>& k;
+        ~Free() {
+            for (void* p : k) cudaFree(p);
+        }
+    } guard{keep};
+    uint64_t* dc = nullptr;
+    LA_TRY(cudaMalloc((void**)&dc, 8 * (size_t)n));
+    keep.push_back(dc);
+    LA_TRY(cudaMemcpyAsync(dc, chunks, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
+    uint64_t* res = nullptr;
+    int64_t rl = 0;
+    if ((rc = radix_combine_run(dc, n, bb, keep, &res, &rl, st))) return rc;
+    // the value is below bb^n < 2^(64n): its limbs are within the first n
+    LA_TRY(cudaMemcpyAsync(out, res, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    LA_TRY(cudaStreamSynchronize(st));
+    int64_t l = n;
+    while (l > 0 && out[l - 1] == 0) l--;
+    *out_len = l;
+    return NBG_OK;
+}

@@ -39,7 +39,7 @@ EXPORTS = [
     "nbg_server_create", "nbg_submit", "nbg_submit_dev", "nbg_poll", "nbg_wait", "nbg_release",
     "nbg_server_stats", "nbg_server_destroy",
     "nbg_powermod_batch", "nbg_powermod_batch_dev", "nbg_barrett_mu", "nbg_powmod_schedule",
-    "nbg_mullo", "nbg_sqrlo", "nbg_matrix22_mul_dev", "nbg_mul2add_dev",
+    "nbg_mullo", "nbg_sqrlo", "nbg_matrix22_mul_dev", "nbg_mul2add_dev", "nbg_radix_combine",
 ]
 
 
@@ -109,6 +109,7 @@ def lib() -> ctypes.CDLL:
             "nbg_powermod_batch": [vp, i64, i64],
             "nbg_mullo": [vp, vp, i64, vp, i64, i64],
             "nbg_matrix22_mul_dev": [vp, i64, vp, i64, vp],
+            "nbg_radix_combine": [vp, i64, vp, i64, c.c_uint64, c.POINTER(i64)],
             "nbg_mul2add_dev": [vp, i64, vp, i64, vp, i64, vp, i64, vp, i64, vp],
             "nbg_sqrlo": [vp, vp, i64, i64],
             "nbg_powermod_batch_dev": [vp, i64, i64, vp],
@@ -231,6 +232,16 @@ def mul2add_dev(r, rn: int, a, la: int, x, lx: int, b, lb: int, y, ly: int, stre
     """r = a*x + b*y on device buffers (cof_mul2!)."""
     _check(lib().nbg_mul2add_dev(_dptr(r), rn, _dptr(a), la, _dptr(x), lx, _dptr(b), lb, _dptr(y), ly,
                                  _stream(stream)))
+
+
+def radix_combine(chunks, bb: int) -> np.ndarray:
+    """Binary limbs of sum(chunks[i] * bb**i) (little-endian chunks < bb), e.g.
+    bb = 10**19 for 19 decimal digits per chunk (radix_combine)."""
+    c = _u64(chunks)
+    out = np.zeros(max(1, c.size), dtype=np.uint64)
+    n = ctypes.c_int64()
+    _check(lib().nbg_radix_combine(_ptr(out), out.size, _ptr(c), c.size, bb, ctypes.byref(n)))
+    return out[: n.value]
 
 
 def mul_batch(pairs) -> list[np.ndarray]:

@@ -703,6 +703,104 @@ def run_powmod(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_single(args) -> None:
+    """Single large products (balanced mul and sqr at 2^16, 2^20, 2^24 limbs;
+    uniform, all-ones and 1%-sparse limbs), each on the plain one-per-call
+    device path (nbg_mul_dev / nbg_sqr_dev: plan lookup, job build, launches)
+    and as a captured one-product batch (graph replay).  >= 20 timed
+    repetitions after warm-up, p50/p99 by CUDA events on the calling stream;
+    roofline = the reference schedule's FP64 instructions / p50 time against
+    the FP64 issue rate measured in this run; GMP mpn_mul/mpn_sqr on one host
+    core beside it (uniform pattern).  One JSON line per case."""
+    import torch
+
+    import nbgpu
+    import oracle
+
+    torch.cuda.set_device(0)
+    nbgpu._check(nbgpu.lib().nbg_init(0))
+    peak = fp64_peak()["dfma_per_s"]
+    s = torch.cuda.Stream()
+    reps = max(20, args.steps)
+    lgs = [int(x) for x in args.single_sizes.split(",")]
+    for lg in lgs:
+        n = 1 << lg
+        for kind in ("uniform", "ones", "sparse"):
+            rng = np.random.Generator(np.random.PCG64(1000 + lg))
+            ops = []
+            for _ in range(2):
+                if kind == "uniform":
+                    x = rng.integers(0, 2**64, n, dtype=np.uint64)
+                elif kind == "ones":
+                    x = np.full(n, 2**64 - 1, dtype=np.uint64)
+                else:
+                    x = np.zeros(n, dtype=np.uint64)
+                    idx = rng.choice(n, n // 100, replace=False)
+                    x[idx] = rng.integers(1, 2**64, idx.size, dtype=np.uint64)
+                x[-1] |= np.uint64(1)
+                ops.append(x)
+            da, db = (torch.from_numpy(x).cuda() for x in ops)
+            for sq in (False, True):
+                r = torch.empty(2 * n, dtype=torch.uint64, device="cuda")
+                ba = 64 * (n - 1) + int(ops[0][-1]).bit_length()
+                bb = ba if sq else 64 * (n - 1) + int(ops[1][-1]).bit_length()
+                descs = nbgpu.make_descs([(r.data_ptr(), da.data_ptr(), None if sq else db.data_ptr(), n, n, ba, bb)])
+                torch.cuda.synchronize()
+
+                def call():
+                    if sq:
+                        nbgpu.sqr_dev(r, da, n, s)
+                    else:
+                        nbgpu.mul_dev(r, da, n, db, n, s)
+
+                def timed(fn):
+                    for _ in range(3):
+                        fn()
+                    torch.cuda.synchronize()
+                    out = []
+                    for _ in range(reps):
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(s)
+                        fn()
+                        e1.record(s)
+                        e1.synchronize()
+                        out.append(e0.elapsed_time(e1))
+                    return out
+
+                t_call = timed(call)
+                bt = nbgpu.Batch(descs)
+                t_graph = timed(lambda: bt.run(s.cuda_stream))
+                alg = sum(x["alg_ops"] for x in bt.stats())
+                bt.close()
+                got = r.cpu().numpy()
+                a0 = ops[0]
+                want = oracle.gmp_sqr(a0) if sq else oracle.gmp_mul(a0, ops[1])
+                if not np.array_equal(got, want):
+                    raise SystemExit(f"single: 2^{lg} {kind} {'sqr' if sq else 'mul'} differs from GMP")
+                gmp_ms = None
+                if kind == "uniform":
+                    t0 = time.perf_counter()
+                    oracle.gmp_sqr(a0) if sq else oracle.gmp_mul(a0, ops[1])
+                    gmp_ms = 1e3 * (time.perf_counter() - t0)
+                p50g = float(np.percentile(t_graph, 50))
+                line = {
+                    "mode": "single", "impl": "ours", "op": "sqr" if sq else "mul", "limbs": n, "pattern": kind,
+                    "metric": "single large product time, bit-exact vs GMP", "unit": "ms", "higher_is_better": False,
+                    "per_call_p50_ms": float(np.percentile(t_call, 50)), "per_call_p99_ms": float(np.percentile(t_call, 99)),
+                    "graph_p50_ms": p50g, "graph_p99_ms": float(np.percentile(t_graph, 99)),
+                    "output_limbs_per_s": 2 * n / (p50g / 1e3),
+                    "roofline": {"bound": "fp64", "alg_ops": alg, "achieved": alg / (p50g / 1e3) / 1e12,
+                                 "peak": peak / 1e12, "unit": "T FP64 instr/s", "frac": alg / (p50g / 1e3) / peak,
+                                 "peak_source": "measured: DFMA issue rate of libnbgpu_peak.so in this run"},
+                    "cpu_baseline": None if gmp_ms is None else {"value": gmp_ms, "unit": "ms", "cores": 1,
+                                                                  "kind": "gmp", "sample": "one call, GMP 6.3 mpn"},
+                    "reps": reps, "dtype": "f64", "data": "synthetic", "n_gpus": 1,
+                }
+                print(json.dumps(line), flush=True)
+            del da, db
+            torch.cuda.empty_cache()
+
+
 def run_route(args) -> None:
     """Per-call time of unbalanced products below the reference's NTT admission
     (smaller operand n < 64: its chunked Karatsuba path) on the GPU (nbg_mul,
@@ -756,6 +854,8 @@ def main() -> None:
     ap.add_argument("--square", action="store_true", help="with --shape: squares of m-limb operands")
     ap.add_argument("--powmod", action="store_true", help="Barrett powermod chains (256-limb moduli)")
     ap.add_argument("--route", action="store_true", help="per-call timings of products below NTT admission")
+    ap.add_argument("--single", action="store_true", help="single large products at --single-sizes")
+    ap.add_argument("--single-sizes", default="16,20,24", help="log2 limb counts")
     ap.add_argument("--powmod-chains", type=int, default=256)
     ap.add_argument("--powmod-ebits", type=int, default=4096, help="exponent bits (a multiple of 64)")
     ap.add_argument("--serve", action="store_true", help="serving loop at swept Poisson arrival rates")
@@ -775,7 +875,10 @@ def main() -> None:
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        if args.route:
+        if args.single:
+            if rank == 0:
+                run_single(args)
+        elif args.route:
             if rank == 0:
                 run_route(args)
         elif args.powmod:

@@ -736,7 +736,8 @@ int nbg_unpack_dev(uint64_t* r, int64_t rn, const double* x1, const double* x2, 
     CUDA_TRY(launch_jobs(JK_UNPACK, (const DProd*)d, E.d_plans, job_list((const Job*)(d + jo)), P.ntl,
                          sizeof(uint64_t) * 2 * align_up((size_t)ncoef, 2), 0, st));
     CUDA_TRY(launch_jobs(JK_CARRY, (const DProd*)d, E.d_plans, job_list((const Job*)(d + jo) + P.ntl), 1, 0, 0, st));
-    g_launches += 2;
+    CUDA_TRY(launch_jobs(JK_CARRYFIX, (const DProd*)d, E.d_plans, job_list((const Job*)(d + jo)), P.ntl, 0, 0, st));
+    g_launches += 3;
     CUDA_TRY(cudaStreamSynchronize(st));
     return NBG_OK;
 }

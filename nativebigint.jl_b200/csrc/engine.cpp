@@ -860,6 +860,9 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         gc.mode = JM_PERPROD;
         gc.njobs = count;
         gc.bytes = carry_bytes;
+        Group& gf = group_of(2 * pmax + 1, JK_CARRYFIX, 0);  // the unpack's tiles again
+        gf.mode = JM_TILES;
+        gf.njobs = (int64_t)aggw;
     }
     // job table: [segments | product list] per launch, then the unpack tile starts
     size_t tb = 0;

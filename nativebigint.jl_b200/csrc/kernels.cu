@@ -23,6 +23,8 @@
 // the grouping changes no bit.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "butterfly.cuh"
 #include "kernels.h"
 
@@ -888,12 +890,41 @@ __global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, 
         for (int64_t k = t0; k < t1; k++) {
             uint32_t a = P.agg[k];
             if (cin) {
-                int64_t w = k * UNPACK_TL, we = min(w + (int64_t)UNPACK_TL, P.rn);
-                while (w < we && P.r[w] == ~0ULL) { P.r[w] = 0; w++; }
-                if (w < we) P.r[w] += 1;
+                // the carry stops at the tile's first limb unless that limb is
+                // all ones; such tiles are left to k_carry_fix, which walks
+                // the run of all-ones limbs with the whole block
+                const int64_t w = k * UNPACK_TL;
+                if (P.r[w] != ~0ULL) P.r[w] += 1;
+                else P.agg[k] = a | 4u;
             }
             cin = (a & 1u) | ((a >> 1) & cin);
         }
+    }
+}
+
+// Tiles that k_carry flagged (bit 2 of their aggregate): the incoming carry
+// runs through the tile's leading all-ones limbs.  One block per flagged tile
+// finds the first limb that is not all ones (it absorbs the +1), zeroing the
+// run before it; a tile that is all ones passes the carry on, which the
+// cross-tile scan already credited to the next tile.  Jobs are the unpack's
+// (product, tile) list; unflagged tiles are skipped at once.
+__global__ void __launch_bounds__(256) k_carry_fix(const DProd* __restrict__ prods, const JobSrc src,
+                                                   int64_t njobs) {
+    __shared__ unsigned long long first;
+    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+        const Job jb = job_at(src, ji);
+        const DProd& P = prods[jb.prod];
+        if (P.ntl <= 1 || !(P.agg[jb.tile] & 4u)) continue;  // uniform across the block
+        const int64_t w0 = jb.tile * UNPACK_TL, we = min(w0 + (int64_t)UNPACK_TL, P.rn);
+        if (threadIdx.x == 0) first = (unsigned long long)we;
+        __syncthreads();
+        for (int64_t w = w0 + threadIdx.x; w < we; w += blockDim.x)
+            if (P.r[w] != ~0ULL) atomicMin(&first, (unsigned long long)w);
+        __syncthreads();
+        const int64_t f = (int64_t)first;
+        for (int64_t w = w0 + threadIdx.x; w < f; w += blockDim.x) P.r[w] = 0;
+        if (threadIdx.x == 0 && f < we) P.r[f] += 1;
+        __syncthreads();
     }
 }
 
@@ -994,6 +1025,12 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
         case JK_REV: k_rev<<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
         case JK_UNPACK: k_unpack<<<grid, UNPACK_THREADS, smem, st>>>(prods, plans, jobs, njobs); break;
         case JK_CARRY: k_carry<<<grid, 256, 0, st>>>(prods, jobs, njobs); break;
+        case JK_CARRYFIX: {
+            // a grid of a few blocks per SM walks the tile list; most tiles are skipped
+            const unsigned g = (unsigned)std::min<int64_t>(njobs, 148 * 8);
+            k_carry_fix<<<g, 256, 0, st>>>(prods, jobs, njobs);
+            break;
+        }
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -173,6 +173,7 @@ enum JobKind : int32_t {
     JK_REV = 2,   // reverse pass
     JK_UNPACK = 3,// Garner + limb assembly + in-tile carries
     JK_CARRY = 4, // cross-tile carry scan and fix-up (one job per product)
+    JK_CARRYFIX = 5, // carries through runs of all-ones limbs (one job per unpack tile)
 };
 
 constexpr int UNPACK_TL = 1024;  // output limbs per unpack tile

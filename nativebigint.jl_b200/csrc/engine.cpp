@@ -794,6 +794,10 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         const double nc = (double)cls.size();
         auto emit = [&](Group& g, const DPass& ps, int nopnd, int sub_base) {
             JobSeg sg;
+            const int64_t per = ps.Qb / ps.C, nblk = ps.ntiles / per;
+            const bool colmajor = per > 1 && nblk > 1;
+            sg.per = colmajor ? (int32_t)per : 0;
+            sg.nblk = colmajor ? (int32_t)nblk : 0;
             sg.begin = g.njobs;
             sg.ntiles = ps.ntiles;
             sg.nop = nopnd;

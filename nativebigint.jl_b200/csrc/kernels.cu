@@ -545,7 +545,11 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_COL_MINB) k_fwd(const DProd*
                                                          const DPlan* __restrict__ plans,
                                                          const JobSrc src, int64_t njobs) {
     extern __shared__ double smem[];
-    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+    // a run of consecutive jobs per CTA: in column passes they share twiddle
+    // columns, which stay in L1 from one tile to the next
+    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
+    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
+    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
         const Job jb = job_at(src, ji);
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
@@ -648,7 +652,11 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_COL_MINB) k_rev(const DProd*
                                                          const DPlan* __restrict__ plans,
                                                          const JobSrc src, int64_t njobs) {
     extern __shared__ double smem[];
-    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+    // a run of consecutive jobs per CTA: in column passes they share twiddle
+    // columns, which stay in L1 from one tile to the next
+    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
+    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
+    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
         const Job jb = job_at(src, ji);
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
@@ -903,28 +911,42 @@ __global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, 
 }
 
 // Tiles that k_carry flagged (bit 2 of their aggregate): the incoming carry
-// runs through the tile's leading all-ones limbs.  One block per flagged tile
-// finds the first limb that is not all ones (it absorbs the +1), zeroing the
-// run before it; a tile that is all ones passes the carry on, which the
-// cross-tile scan already credited to the next tile.  Jobs are the unpack's
-// (product, tile) list; unflagged tiles are skipped at once.
+// runs through the tile's leading all-ones limbs.  For each flagged tile the
+// whole block finds the first limb that is not all ones (it absorbs the +1),
+// zeroing the run before it; a tile that is all ones passes the carry on,
+// which the cross-tile scan already credited to the next tile.  Jobs are the
+// unpack's (product, tile) list, checked 256 at a time (one per thread).
 __global__ void __launch_bounds__(256) k_carry_fix(const DProd* __restrict__ prods, const JobSrc src,
                                                    int64_t njobs) {
     __shared__ unsigned long long first;
-    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const Job jb = job_at(src, ji);
-        const DProd& P = prods[jb.prod];
-        if (P.ntl <= 1 || !(P.agg[jb.tile] & 4u)) continue;  // uniform across the block
-        const int64_t w0 = jb.tile * UNPACK_TL, we = min(w0 + (int64_t)UNPACK_TL, P.rn);
-        if (threadIdx.x == 0) first = (unsigned long long)we;
+    __shared__ int nflag;
+    __shared__ int64_t flagged[256];
+    // the block checks 256 tiles at once (one per thread) and walks the flagged ones
+    for (int64_t j0 = (int64_t)blockIdx.x * blockDim.x; j0 < njobs; j0 += (int64_t)gridDim.x * blockDim.x) {
+        if (threadIdx.x == 0) nflag = 0;
         __syncthreads();
-        for (int64_t w = w0 + threadIdx.x; w < we; w += blockDim.x)
-            if (P.r[w] != ~0ULL) atomicMin(&first, (unsigned long long)w);
+        const int64_t ji = j0 + threadIdx.x;
+        if (ji < njobs) {
+            const Job jb = job_at(src, ji);
+            const DProd& P = prods[jb.prod];
+            if (P.ntl > 1 && (P.agg[jb.tile] & 4u)) flagged[atomicAdd(&nflag, 1)] = ji;
+        }
         __syncthreads();
-        const int64_t f = (int64_t)first;
-        for (int64_t w = w0 + threadIdx.x; w < f; w += blockDim.x) P.r[w] = 0;
-        if (threadIdx.x == 0 && f < we) P.r[f] += 1;
-        __syncthreads();
+        const int nf = nflag;
+        for (int f = 0; f < nf; f++) {
+            const Job jb = job_at(src, flagged[f]);
+            const DProd& P = prods[jb.prod];
+            const int64_t w0 = jb.tile * UNPACK_TL, we = min(w0 + (int64_t)UNPACK_TL, P.rn);
+            if (threadIdx.x == 0) first = (unsigned long long)we;
+            __syncthreads();
+            for (int64_t w = w0 + threadIdx.x; w < we; w += blockDim.x)
+                if (P.r[w] != ~0ULL) atomicMin(&first, (unsigned long long)w);
+            __syncthreads();
+            const int64_t fw = (int64_t)first;
+            for (int64_t w = w0 + threadIdx.x; w < fw; w += blockDim.x) P.r[w] = 0;
+            if (threadIdx.x == 0 && fw < we) P.r[fw] += 1;
+            __syncthreads();
+        }
     }
 }
 
@@ -1016,6 +1038,11 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
                         size_t smem, int grid_cap, cudaStream_t st) {
     if (njobs <= 0) return cudaSuccess;
     int64_t grid64 = njobs;
+    if (kind == JK_FWD || kind == JK_REV) {
+        // up to 8 consecutive jobs per CTA while keeping >= 4 waves of 3 CTAs per SM
+        const int64_t k = std::max<int64_t>(1, std::min<int64_t>(8, njobs / (148 * 3 * 4)));
+        grid64 = (njobs + k - 1) / k;
+    }
     if (grid_cap > 0 && grid64 > grid_cap) grid64 = grid_cap;
     if (grid64 > 0x7fffffff) grid64 = 0x7fffffff;
     const unsigned grid = (unsigned)grid64;
@@ -1026,8 +1053,8 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
         case JK_UNPACK: k_unpack<<<grid, UNPACK_THREADS, smem, st>>>(prods, plans, jobs, njobs); break;
         case JK_CARRY: k_carry<<<grid, 256, 0, st>>>(prods, jobs, njobs); break;
         case JK_CARRYFIX: {
-            // a grid of a few blocks per SM walks the tile list; most tiles are skipped
-            const unsigned g = (unsigned)std::min<int64_t>(njobs, 148 * 8);
+            // each block checks 256 tiles per step; most tiles are skipped
+            const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((njobs + 255) / 256, 148 * 8));
             k_carry_fix<<<g, 256, 0, st>>>(prods, jobs, njobs);
             break;
         }

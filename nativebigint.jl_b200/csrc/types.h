@@ -101,6 +101,11 @@ struct JobSeg {
     int64_t ntiles;
     int32_t nop, nprod;
     int32_t first, sub_base;
+    // column passes: tiles are visited column-major, so consecutive jobs (and
+    // the jobs one CTA runs in a row) read the same twiddle columns: the
+    // t-th visited tile is (t % nblk) * per + t / nblk, per = tiles per block
+    // row (Qb / C), nblk = ntiles / per.  per = 0: tiles in index order.
+    int32_t per, nblk;
 };
 
 // Where a launch's jobs come from.  Batches describe them implicitly, so the
@@ -163,7 +168,7 @@ NBG_HD inline Job job_at(const JobSrc& s, int64_t ji) {
     const int32_t op = (int32_t)(r / g.nprod);
     j.prod = s.plist[g.first + (int32_t)(r - (int64_t)op * g.nprod)];
     j.sub = g.sub_base | (op << 1);
-    j.tile = t;
+    j.tile = g.per ? (t % g.nblk) * g.per + t / g.nblk : t;
     return j;
 }
 

@@ -61,7 +61,7 @@ int check_desc(const nbg_desc& d, ProdIn& q, bool host) {
 namespace {
 
 constexpr size_t CHUNK_BYTES = size_t(64) << 20;
-constexpr int NBUF = 2;
+constexpr int NBUF = 3;
 
 struct Span {
     const char* h;  // host start
@@ -189,7 +189,20 @@ int host_batch(const nbg_desc* descs, int64_t count) {
             if (cudaStreamWaitEvent(E.copy_in, ev_out[buf], 0) != cudaSuccess) { rc = fail(NBG_ECUDA, "wait"); break; }
         }
         const size_t base_in = align_up(c.bb.dev_bytes, 256);
-        if ((rc = upload_batch(E, c.bb, base, E.copy_in))) break;
+        // descriptors and job table through the region's pinned staging buffer
+        // (an asynchronous copy: the host runs ahead to the next chunk); the
+        // buffer's previous chunk must have been copied out of it first
+        if (ci >= (size_t)nbuf && cudaEventSynchronize(ev_in[buf]) != cudaSuccess) {
+            rc = fail(NBG_ECUDA, "staging wait");
+            break;
+        }
+        if ((rc = E.ensure_stage(buf, c.bb.head_bytes))) break;
+        bind_batch(c.bb, base);
+        stage_batch(c.bb, E.stage[buf]);
+        if (cudaMemcpyAsync(base, E.stage[buf], c.bb.head_bytes, cudaMemcpyHostToDevice, E.copy_in) != cudaSuccess) {
+            rc = fail(NBG_ECUDA, "descriptor copy failed");
+            break;
+        }
         for (const Span& sp : c.in_spans)
             if (cudaMemcpyAsync(base + base_in + sp.d, sp.h, sp.n, cudaMemcpyHostToDevice, E.copy_in) != cudaSuccess) {
                 rc = fail(NBG_ECUDA, "operand copy failed");

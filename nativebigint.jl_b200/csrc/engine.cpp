@@ -647,6 +647,20 @@ void Engine::trim_plans() {
     plan_used = 0;
 }
 
+int Engine::ensure_stage(int i, size_t bytes) {
+    if (bytes <= stage_bytes[i]) return NBG_OK;
+    if (stage[i]) cudaFreeHost(stage[i]);
+    stage[i] = nullptr;
+    stage_bytes[i] = 0;
+    const size_t want = std::max(bytes + bytes / 4, (size_t)1 << 20);
+    if (cudaMallocHost((void**)&stage[i], want) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NBG_ENOMEM, "pinned staging of %zu bytes unavailable", want);
+    }
+    stage_bytes[i] = want;
+    return NBG_OK;
+}
+
 int Engine::ensure_pool(size_t bytes) {
     if (bytes <= pool_bytes) return NBG_OK;
     if (pool) {

@@ -73,6 +73,9 @@ struct Engine {
     int plan_used = 0;
     void* pool = nullptr;
     size_t pool_bytes = 0;
+    // pinned staging for the descriptor/job-table head of each pipelined chunk
+    char* stage[4] = {};
+    size_t stage_bytes[4] = {};
 
     int init(int device);
     int ensure();
@@ -81,6 +84,7 @@ struct Engine {
     void drop_plans();
     void trim_plans();  // frees every plan's tables: no batch may exist or be running
     int ensure_pool(size_t bytes);
+    int ensure_stage(int i, size_t bytes);
 };
 extern Engine g_eng;
 

@@ -60,7 +60,7 @@ int check_desc(const nbg_desc& d, ProdIn& q, bool host) {
 
 namespace {
 
-constexpr size_t CHUNK_BYTES = size_t(64) << 20;
+constexpr size_t CHUNK_BYTES = size_t(128) << 20;
 constexpr int NBUF = 3;
 
 struct Span {
@@ -123,7 +123,7 @@ int host_batch(const nbg_desc* descs, int64_t count) {
         if (rc) return rc;
     }
     // chunks of ~CHUNK_BYTES operands, in input order
-    std::vector<Chunk> chunks;
+    std::vector<std::pair<int64_t, int64_t>> bounds;  // (start, count)
     {
         size_t acc = 0;
         int64_t st = 0;
@@ -131,19 +131,43 @@ int host_batch(const nbg_desc* descs, int64_t count) {
             const ProdIn& q = in[(size_t)k];
             acc += 8 * (size_t)(q.m + (q.sqr ? 0 : q.n));
             if (acc >= CHUNK_BYTES || k == count - 1) {
-                Chunk c;
-                c.start = st;
-                c.count = k + 1 - st;
-                chunks.push_back(std::move(c));
+                bounds.push_back({st, k + 1 - st});
                 st = k + 1;
                 acc = 0;
             }
         }
     }
-    size_t region = 0;
-    for (Chunk& c : chunks) {
-        int rc = build_batch(E, in.data() + c.start, c.count, c.bb);
-        if (rc) return rc;
+    // Each chunk is built on the host while the chunks before it copy and
+    // compute; its device region comes from the stream-ordered allocator and
+    // goes back after its results are copied out.  At most NBUF chunks are in
+    // flight (the host waits for the oldest before starting another).
+    cudaEvent_t ev_in[NBUF], ev_comp[NBUF], ev_out[NBUF];
+    for (int i = 0; i < NBUF; i++) {
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_comp[i], cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev_out[i], cudaEventDisableTiming));
+    }
+    {
+        // keep freed chunk regions in the device's memory pool for the next call
+        // instead of returning them to the driver at each synchronization
+        static int tuned_dev = -1;
+        if (tuned_dev != E.dev) {
+            cudaMemPool_t mp;
+            if (cudaDeviceGetDefaultMemPool(&mp, E.dev) == cudaSuccess) {
+                uint64_t thr = UINT64_MAX;
+                cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
+            }
+            cudaGetLastError();
+            tuned_dev = E.dev;
+        }
+    }
+    int rc = NBG_OK;
+    for (size_t ci = 0; ci < bounds.size() && rc == NBG_OK; ci++) {
+        const int buf = (int)(ci % (size_t)NBUF);
+        Chunk c;
+        c.start = bounds[ci].first;
+        c.count = bounds[ci].second;
+        if ((rc = build_batch(E, in.data() + c.start, c.count, c.bb))) break;
         std::vector<std::pair<const char*, size_t>> ir, orr;
         for (int64_t k = 0; k < c.count; k++) {
             const ProdIn& q = in[(size_t)(c.start + k)];
@@ -155,47 +179,27 @@ int host_batch(const nbg_desc* descs, int64_t count) {
         c.in_bytes = layout_spans(ir, 0, c.in_spans, ioff);
         c.out_bytes = layout_spans(orr, 0, c.out_spans, ooff);
         const size_t base_in = align_up(c.bb.dev_bytes, 256), base_out = base_in + c.in_bytes;
+        c.region = align_up(base_out + c.out_bytes, 256);
+        // the slot's previous chunk: its staging buffer and its events are reused
+        if (ci >= (size_t)NBUF && cudaEventSynchronize(ev_out[buf]) != cudaSuccess) {
+            rc = fail(NBG_ECUDA, "pipeline wait");
+            break;
+        }
+        char* base = nullptr;
+        if (cudaMallocAsync((void**)&base, c.region, E.copy_in) != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(NBG_ENOMEM, "device region of %zu bytes unavailable", c.region);
+            break;
+        }
         size_t ii = 0;
         for (int64_t k = 0; k < c.count; k++) {
             const ProdIn& q = in[(size_t)(c.start + k)];
             DProd& P = c.bb.prods[(size_t)k];
-            // device addresses are relative to the region; made absolute below
-            P.a = (const uint64_t*)(uintptr_t)(base_in + ioff[ii++]);
-            P.b = q.sqr ? P.a : (const uint64_t*)(uintptr_t)(base_in + ioff[ii++]);
-            P.r = (uint64_t*)(uintptr_t)(base_out + ooff[(size_t)k]);
+            P.a = (const uint64_t*)(base + base_in + ioff[ii++]);
+            P.b = q.sqr ? P.a : (const uint64_t*)(base + base_in + ioff[ii++]);
+            P.r = (uint64_t*)(base + base_out + ooff[(size_t)k]);
         }
-        c.region = align_up(base_out + c.out_bytes, 256);
-        region = std::max(region, c.region);
-    }
-    const int nbuf = std::min<int>(NBUF, (int)chunks.size());
-    int rc = E.ensure_pool(region * (size_t)nbuf);
-    if (rc) return rc;
-    cudaEvent_t ev_in[NBUF], ev_comp[NBUF], ev_out[NBUF];
-    for (int i = 0; i < NBUF; i++) {
-        CUDA_TRY(cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming));
-        CUDA_TRY(cudaEventCreateWithFlags(&ev_comp[i], cudaEventDisableTiming));
-        CUDA_TRY(cudaEventCreateWithFlags(&ev_out[i], cudaEventDisableTiming));
-    }
-    for (size_t ci = 0; ci < chunks.size() && rc == NBG_OK; ci++) {
-        Chunk& c = chunks[ci];
-        const int buf = (int)(ci % (size_t)nbuf);
-        char* base = (char*)E.pool + (size_t)buf * region;
-        for (DProd& P : c.bb.prods) {
-            P.a = (const uint64_t*)(base + (uintptr_t)P.a);
-            P.b = (const uint64_t*)(base + (uintptr_t)P.b);
-            P.r = (uint64_t*)(base + (uintptr_t)P.r);
-        }
-        if (ci >= (size_t)nbuf) {  // the region's previous chunk must be fully drained
-            if (cudaStreamWaitEvent(E.copy_in, ev_out[buf], 0) != cudaSuccess) { rc = fail(NBG_ECUDA, "wait"); break; }
-        }
-        const size_t base_in = align_up(c.bb.dev_bytes, 256);
-        // descriptors and job table through the region's pinned staging buffer
-        // (an asynchronous copy: the host runs ahead to the next chunk); the
-        // buffer's previous chunk must have been copied out of it first
-        if (ci >= (size_t)nbuf && cudaEventSynchronize(ev_in[buf]) != cudaSuccess) {
-            rc = fail(NBG_ECUDA, "staging wait");
-            break;
-        }
+        // descriptors and job table through the slot's pinned staging buffer
         if ((rc = E.ensure_stage(buf, c.bb.head_bytes))) break;
         bind_batch(c.bb, base);
         stage_batch(c.bb, E.stage[buf]);
@@ -214,7 +218,6 @@ int host_batch(const nbg_desc* descs, int64_t count) {
         if ((rc = run_launches(E, c.bb, base, E.stream))) break;
         cudaEventRecord(ev_comp[buf], E.stream);
         cudaStreamWaitEvent(E.copy_out, ev_comp[buf], 0);
-        const size_t base_out = base_in + c.in_bytes;
         for (const Span& sp : c.out_spans)
             if (cudaMemcpyAsync((void*)sp.h, base + base_out + sp.d, sp.n, cudaMemcpyDeviceToHost, E.copy_out) !=
                 cudaSuccess) {
@@ -222,6 +225,7 @@ int host_batch(const nbg_desc* descs, int64_t count) {
                 break;
             }
         if (rc) break;
+        cudaFreeAsync(base, E.copy_out);
         cudaEventRecord(ev_out[buf], E.copy_out);
     }
     cudaError_t e1 = cudaStreamSynchronize(E.copy_in);

@@ -35,9 +35,8 @@
 #ifndef NBG_PWR_MINB
 #define NBG_PWR_MINB 3
 #endif
-#ifndef NBG_COL_MINB
-#define NBG_COL_MINB 3
-#endif
+// Column passes with tile sets up to this size run the 4-CTA/SM build.
+constexpr size_t COL4_MAX_SMEM = 32 * 1024;
 // Rounds are inlined into the kernels; out-of-line rounds (NBG_ROUND_NOINLINE)
 // measured 40% slower in k_pwr.
 #ifdef NBG_ROUND_NOINLINE
@@ -541,7 +540,10 @@ __device__ __forceinline__ Tiles make_tiles(double* s, int stride, int ntiles, i
 
 // ---------------------------------------------------------------------------
 // Forward pass of one tile of one operand, both primes (tiles X0, X1).
-__global__ void __launch_bounds__(PASS_THREADS, NBG_COL_MINB) k_fwd(const DProd* __restrict__ prods,
+// MINB: CTAs per SM the register budget is cut for (3: 80 registers, 4: 64);
+// launches pick 4 when the tile set is small enough for four CTAs' shared memory.
+template <int MINB>
+__global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const JobSrc src, int64_t njobs) {
     extern __shared__ double smem[];
@@ -648,7 +650,8 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
 }
 
 // Reverse pass of one tile, both primes.
-__global__ void __launch_bounds__(PASS_THREADS, NBG_COL_MINB) k_rev(const DProd* __restrict__ prods,
+template <int MINB>
+__global__ void __launch_bounds__(PASS_THREADS, MINB) k_rev(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const JobSrc src, int64_t njobs) {
     extern __shared__ double smem[];
@@ -1019,7 +1022,8 @@ cudaError_t kernels_init(double p1, double p2) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const void* ks[] = {(const void*)k_fwd, (const void*)k_pwr, (const void*)k_rev, (const void*)k_unpack};
+    const void* ks[] = {(const void*)k_fwd<3>, (const void*)k_fwd<4>, (const void*)k_pwr,
+                        (const void*)k_rev<3>, (const void*)k_rev<4>, (const void*)k_unpack};
     for (const void* k : ks) {
         cudaFuncAttributes fa;
         e = cudaFuncGetAttributes(&fa, k);
@@ -1047,9 +1051,15 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
     if (grid64 > 0x7fffffff) grid64 = 0x7fffffff;
     const unsigned grid = (unsigned)grid64;
     switch (kind) {
-        case JK_FWD: k_fwd<<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_FWD:
+            if (smem <= COL4_MAX_SMEM) k_fwd<4><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
+            else k_fwd<3><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
+            break;
         case JK_PWR: k_pwr<<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
-        case JK_REV: k_rev<<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_REV:
+            if (smem <= COL4_MAX_SMEM) k_rev<4><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
+            else k_rev<3><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
+            break;
         case JK_UNPACK: k_unpack<<<grid, UNPACK_THREADS, smem, st>>>(prods, plans, jobs, njobs); break;
         case JK_CARRY: k_carry<<<grid, 256, 0, st>>>(prods, jobs, njobs); break;
         case JK_CARRYFIX: {

@@ -793,6 +793,15 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         return bb.prods[(size_t)x].plan < bb.prods[(size_t)y].plan;
     });
     std::vector<int32_t> cls;
+    // A batch whose last-pass tiles are fewer than one wave of CTAs (3 per SM)
+    // gives each prime of a tile its own CTA: twice the CTAs, half the
+    // critical path each (small batches are latency-bound).
+    int64_t pwr_tiles = 0;
+    for (int64_t k = 0; k < count; k++) {
+        const DPlan& pl = bb.plan_of[(size_t)k]->d;
+        pwr_tiles += pl.pass[pl.npass - 1].ntiles;
+    }
+    const bool split_pwr = pwr_tiles < 3 * (int64_t)std::max(E.num_sms, 1);
     for (size_t i = 0; i < byclass.size();) {
         const int slot = bb.prods[(size_t)byclass[i]].plan;
         cls.clear();
@@ -836,11 +845,15 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         }
         {
             const DPass& ps = pl.pass[Pn - 1];
-            const size_t smem = sizeof(double) * (P0.sqr ? 2 : 4) * (size_t)tile_stride_doubles(ps.G * ps.C);
+            // splitting pays only where a tile set holds more 16-point units
+            // than a CTA has threads (smaller tiles just repeat the pack)
+            const bool split = split_pwr && (int64_t)ps.G * ps.C * 2 * nop > 16 * PASS_THREADS;
+            const size_t smem = sizeof(double) * (P0.sqr ? 1 : 2) * (split ? 1 : 2) *
+                                (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
-            const double jobs = (double)ps.ntiles * nc;
-            Group& g = group_of(pmax - 1, JK_PWR, smem);
-            emit(g, ps, 1, (Pn - 1) << 8);
+            const double jobs = (double)ps.ntiles * nc;  // tiles of both primes (the work, split or not)
+            Group& g = group_of(pmax - 1, split ? JK_PWR_SPLIT : JK_PWR, smem);
+            emit(g, ps, split ? 2 : 1, (Pn - 1) << 8);  // split: "operand" is the prime
             g.ops += jobs * 2.0 * (nop * pass_ops(pl, ps, true) + 7.0 * pts + pass_ops(pl, ps, false));
             const double in_b = Pn == 1 ? (double)ps.ntiles * nop * pts * sum_bch / 8.0 : jobs * 2.0 * nop * 8.0 * pts;
             g.bytes += in_b + jobs * 2.0 * 8.0 * pts;

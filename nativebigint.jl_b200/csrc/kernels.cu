@@ -87,6 +87,7 @@ struct Tiles {
     int lc;   // log2 C
     int Qb;   // pass column stride (global)
     int j0;   // first global column of the tile
+    int pfix; // -1: tile t is prime t >> pshift; 0 or 1: every tile is that prime
 };
 
 // unit u of a round over all tiles -> (tile, unit within tile)
@@ -119,7 +120,7 @@ __device__ NBG_ROUND void round_gen(const Tiles& T, const DStage& st) {
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
         int tau;
         const int uu = split_unit(u, per, tau);
-        const bool p1 = (tau >> T.pshift) != 0;
+        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : (tau >> T.pshift) != 0;
         const Fp F = p1 ? F1 : F0;
         double* s = T.s + tau * T.stride;
         const int c = uu & (C - 1);
@@ -169,7 +170,7 @@ __device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStag
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
         int tau;
         const int uu = split_unit(u, per, tau);
-        const bool p1 = (tau >> T.pshift) != 0;
+        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : (tau >> T.pshift) != 0;
         const Fp F = fpctx(p1 ? 1 : 0);
         const double wi = p1 ? wi1 : wi0;
         double* s = T.s + tau * T.stride;
@@ -230,7 +231,7 @@ __device__ NBG_ROUND void round_r8(const Tiles& T, const DStage& A) {
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
         int tau;
         const int b = split_unit(u, per, tau);
-        const bool p1 = (tau >> T.pshift) != 0;
+        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : (tau >> T.pshift) != 0;
         const Fp F = p1 ? F1 : F0;
         const double wi = p1 ? wi1 : wi0;
         double* s = T.s + tau * T.stride;
@@ -271,6 +272,7 @@ struct FuseTiles {
     int stride;
     int sq;
     int G, lc, Qb, j0;
+    int pfix;  // -1: tiles of both primes; 0 or 1: only that prime's (a, b) tiles
 };
 
 __device__ __forceinline__ void pw4(double* a, const double* b, Fp F) {
@@ -312,15 +314,15 @@ __device__ NBG_ROUND void fused_r16(const FuseTiles& T, const DStage& A, const D
     const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
     const int QA = (int)A.Q, QB = (int)B.Q;
     const int per = (T.G >> 4) << T.lc;
-    const int total = 2 * per;
+    const int total = T.pfix >= 0 ? per : 2 * per;
     const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
     const double *twA0 = A.tw[0], *twA1 = A.tw[1], *twB0 = B.tw[0], *twB1 = B.tw[1];
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
-        const bool p1 = u >= per;
-        const int uu = p1 ? u - per : u;
+        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : u >= per;
+        const int uu = (T.pfix < 0 && p1) ? u - per : u;
         const Fp F = fpctx(p1 ? 1 : 0);
         const double wi = p1 ? wi1 : wi0;
-        double* sa = T.s + (p1 ? (T.sq ? 1 : 2) : 0) * T.stride;
+        double* sa = T.s + ((T.pfix < 0 && p1) ? (T.sq ? 1 : 2) : 0) * T.stride;
         double* sb = T.sq ? sa : sa + T.stride;
         const int c = uu & (C - 1);
         const int r = uu >> T.lc;
@@ -362,15 +364,15 @@ __device__ NBG_ROUND void fused_r16(const FuseTiles& T, const DStage& A, const D
 
 __device__ NBG_ROUND void fused_r8(const FuseTiles& T, const DStage& A) {
     const int per = T.G >> 3;
-    const int total = 2 * per;
+    const int total = T.pfix >= 0 ? per : 2 * per;
     const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
     const double *tw0 = A.tw[0], *tw1 = A.tw[1];
     for (int u = threadIdx.x; u < total; u += blockDim.x) {
-        const bool p1 = u >= per;
-        const int b = p1 ? u - per : u;
+        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : u >= per;
+        const int b = (T.pfix < 0 && p1) ? u - per : u;
         const Fp F = fpctx(p1 ? 1 : 0);
         const double wi = p1 ? wi1 : wi0;
-        double* sa = T.s + (p1 ? (T.sq ? 1 : 2) : 0) * T.stride;
+        double* sa = T.s + ((T.pfix < 0 && p1) ? (T.sq ? 1 : 2) : 0) * T.stride;
         double* sb = T.sq ? sa : sa + T.stride;
         const double* tw = p1 ? tw1 : tw0;
         const double w0[4] = {0.0, __ldg(tw + 0), __ldg(tw + 2), __ldg(tw + 4)};
@@ -535,6 +537,7 @@ __device__ __forceinline__ Tiles make_tiles(double* s, int stride, int ntiles, i
     T.lc = __ffs(ps.C) - 1;
     T.Qb = (int)ps.Qb;
     T.j0 = j0;
+    T.pfix = -1;
     return T;
 }
 
@@ -581,6 +584,7 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restr
 
 // Last pass, both primes: forward on a (and b), pointwise, reverse on a.
 // Tiles: products [a0, b0, a1, b1], squares [a0, a1].
+template <bool SPLIT>
 __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const JobSrc src, int64_t njobs) {
@@ -595,29 +599,38 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
         tile_geo(pl, ps, jb.tile, base, j0);
         const int stride = tile_stride_doubles(ps.G * ps.C);
         const int sq = P.sqr;
+        // split launches (JK_PWR_SPLIT) give each prime (sub bit 1) its own
+        // CTA: half the tiles, twice the CTAs, for batches too small to fill
+        // the GPU
+        const int pf = SPLIT ? (jb.sub >> 1) & 1 : -1;
         double* a0 = smem;
         double* a1 = smem + (sq ? 1 : 2) * stride;
         double* b0 = sq ? a0 : smem + stride;
         double* b1 = sq ? a1 : smem + 3 * stride;
+        const int p0 = pf >= 0 ? pf : 0;
         const int cnt = ps.G * ps.C;
         __syncthreads();
         if (pass == 0 && !(P.flags & PF_PRELOADED)) {
-            pack_tile2(a0, a1, P.a, P.m, P.bch, P.nca, ps, base);
-            if (!sq) pack_tile2(b0, b1, P.b, P.n, P.bch, P.ncb, ps, base);
+            pack_tile2(a0, pf >= 0 ? a0 : a1, P.a, P.m, P.bch, P.nca, ps, base);
+            if (!sq) pack_tile2(b0, pf >= 0 ? b0 : b1, P.b, P.n, P.bch, P.ncb, ps, base);
         } else {
-            load_tile_async(a0, P.xa[0], ps, base);
-            load_tile_async(a1, P.xa[1], ps, base);
-            if (!sq) {
-                load_tile_async(b0, P.xb[0], ps, base);
-                load_tile_async(b1, P.xb[1], ps, base);
+            load_tile_async(a0, P.xa[p0], ps, base);
+            if (!sq) load_tile_async(b0, P.xb[p0], ps, base);
+            if (pf < 0) {
+                load_tile_async(a1, P.xa[1], ps, base);
+                if (!sq) load_tile_async(b1, P.xb[1], ps, base);
             }
             cp_async_wait_all();
         }
+        Tiles TF = pf < 0 ? make_tiles(smem, stride, sq ? 2 : 4, sq ? 0 : 1, ps, j0)
+                          : make_tiles(smem, stride, sq ? 1 : 2, 30, ps, j0);
+        Tiles TR = pf < 0 ? make_tiles(a0, (int)(a1 - a0), 2, 0, ps, j0) : make_tiles(a0, stride, 1, 30, ps, j0);
+        TF.pfix = pf;
+        TR.pfix = pf;
         const int nr = ps.nrounds;
         const int lastk = ps.rkind[nr - 1];
         if (lastk == RK_R16 || lastk == RK_R8) {
             // forward rounds but the last, fused round, reverse rounds but the first
-            const Tiles TF = make_tiles(smem, stride, sq ? 2 : 4, sq ? 0 : 1, ps, j0);
             for (int r = 0; r < nr - 1; r++) run_round<true>(TF, pl, ps.rkind[r], ps.rstage[r]);
             __syncthreads();
             FuseTiles FT;
@@ -628,24 +641,32 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
             FT.lc = __ffs(ps.C) - 1;
             FT.Qb = (int)ps.Qb;
             FT.j0 = j0;
+            FT.pfix = pf;
             const int s0 = ps.rstage[nr - 1];
             if (lastk == RK_R16) fused_r16(FT, pl.st[s0], pl.st[s0 + 1]);
             else fused_r8(FT, pl.st[s0]);
-            const Tiles TR = make_tiles(a0, (int)(a1 - a0), 2, 0, ps, j0);
             for (int r = nr - 2; r >= 0; r--) run_round<false>(TR, pl, ps.rkind[r], ps.rstage[r]);
             __syncthreads();
         } else {
-            run_pass<true>(make_tiles(smem, stride, sq ? 2 : 4, sq ? 0 : 1, ps, j0), pl, ps);
-            const Fp F0 = fpctx(0), F1 = fpctx(1);
-            for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
-                const int i = sp(e);
-                a0[i] = fp_mulmod(a0[i], b0[i], F0);
-                a1[i] = fp_mulmod(a1[i], b1[i], F1);
+            run_pass<true>(TF, pl, ps);
+            if (pf < 0) {
+                const Fp F0 = fpctx(0), F1 = fpctx(1);
+                for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+                    const int i = sp(e);
+                    a0[i] = fp_mulmod(a0[i], b0[i], F0);
+                    a1[i] = fp_mulmod(a1[i], b1[i], F1);
+                }
+            } else {
+                const Fp F = fpctx(pf);
+                for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+                    const int i = sp(e);
+                    a0[i] = fp_mulmod(a0[i], b0[i], F);
+                }
             }
-            run_pass<false>(make_tiles(a0, (int)(a1 - a0), 2, 0, ps, j0), pl, ps);
+            run_pass<false>(TR, pl, ps);
         }
-        store_tile(a0, P.xa[0], ps, base);
-        store_tile(a1, P.xa[1], ps, base);
+        store_tile(a0, P.xa[p0], ps, base);
+        if (pf < 0) store_tile(a1, P.xa[1], ps, base);
     }
 }
 
@@ -1022,7 +1043,7 @@ cudaError_t kernels_init(double p1, double p2) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const void* ks[] = {(const void*)k_fwd<3>, (const void*)k_fwd<4>, (const void*)k_pwr,
+    const void* ks[] = {(const void*)k_fwd<3>, (const void*)k_fwd<4>, (const void*)k_pwr<false>, (const void*)k_pwr<true>,
                         (const void*)k_rev<3>, (const void*)k_rev<4>, (const void*)k_unpack};
     for (const void* k : ks) {
         cudaFuncAttributes fa;
@@ -1055,7 +1076,8 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
             if (smem <= COL4_MAX_SMEM) k_fwd<4><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
             else k_fwd<3><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
             break;
-        case JK_PWR: k_pwr<<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_PWR: k_pwr<false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_PWR_SPLIT: k_pwr<true><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
         case JK_REV:
             if (smem <= COL4_MAX_SMEM) k_rev<4><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
             else k_rev<3><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);

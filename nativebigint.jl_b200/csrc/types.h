@@ -179,6 +179,7 @@ enum JobKind : int32_t {
     JK_UNPACK = 3,// Garner + limb assembly + in-tile carries
     JK_CARRY = 4, // cross-tile carry scan and fix-up (one job per product)
     JK_CARRYFIX = 5, // carries through runs of all-ones limbs (one job per unpack tile)
+    JK_PWR_SPLIT = 6,// JK_PWR with one job per prime (sub bit 1) for small batches
 };
 
 constexpr int UNPACK_TL = 1024;  // output limbs per unpack tile

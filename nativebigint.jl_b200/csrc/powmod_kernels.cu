@@ -89,7 +89,7 @@ __device__ uint64_t warp_sub(uint64_t* x, const uint64_t* u, const uint64_t* v, 
 __device__ int warp_geq(const uint64_t* x, const uint64_t* v, int64_t n, int64_t nv, int lane) {
     const int64_t per = (n + 31) / 32;
     const int64_t j0 = (int64_t)lane * per, j1 = min(j0 + per, n);
-    int cmp = 0;  // this lane's verdict from its highest differing limb
+    int cmp = 0;  // this lane's answer from its highest differing limb
     for (int64_t j = j1 - 1; j >= j0; j--) {
         const uint64_t a = x[j], b = j < nv ? v[j] : 0;
         if (a != b) {

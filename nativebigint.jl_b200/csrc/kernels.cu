@@ -548,14 +548,14 @@ __device__ __forceinline__ Tiles make_tiles(double* s, int stride, int ntiles, i
 template <int MINB>
 __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
-                                                         const JobSrc src, int64_t njobs) {
+                                                         const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];
     // a run of consecutive jobs per CTA: in column passes they share twiddle
     // columns, which stay in L1 from one tile to the next
     const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
     const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
     for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
-        const Job jb = job_at(src, ji);
+        const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int opb = (jb.sub >> 1) & 1, pass = (jb.sub >> 8) & 0xff;
@@ -587,10 +587,10 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restr
 template <bool SPLIT>
 __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
-                                                         const JobSrc src, int64_t njobs) {
+                                                         const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const Job jb = job_at(src, ji);
+        const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int pass = P.npass - 1;
@@ -674,14 +674,14 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
 template <int MINB>
 __global__ void __launch_bounds__(PASS_THREADS, MINB) k_rev(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
-                                                         const JobSrc src, int64_t njobs) {
+                                                         const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];
     // a run of consecutive jobs per CTA: in column passes they share twiddle
     // columns, which stay in L1 from one tile to the next
     const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
     const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
     for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
-        const Job jb = job_at(src, ji);
+        const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int pass = (jb.sub >> 8) & 0xff;
@@ -781,12 +781,12 @@ __device__ __forceinline__ void limb_range(int64_t w, int b, double rb, int64_t 
 
 __global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restrict__ prods,
                                                            const DPlan* __restrict__ plans,
-                                                           const JobSrc src, int64_t njobs) {
+                                                           const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ uint64_t usm[];
     __shared__ uint32_t wagg[UNPACK_THREADS / 32];
     __shared__ uint64_t hilast[UNPACK_THREADS + 1];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const Job jb = job_at(src, ji);
+        const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int b = P.bch;
@@ -892,11 +892,11 @@ __global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restri
 // Cross-tile carries: one CTA per product.  Each thread composes a run of
 // tile aggregates, the block scans them, and every tile whose true carry-in is
 // 1 gets +1 propagated from its first limb (limbs equal to 2^64-1 wrap to 0).
-__global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, const JobSrc src,
+__global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, const Job* __restrict__ jobs,
                                                int64_t njobs) {
     __shared__ uint32_t wagg[8];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const DProd& P = prods[job_at(src, ji).prod];
+        const DProd& P = prods[jobs[ji].prod];
         const int64_t nt = P.ntl;
         if (nt <= 1) continue;  // one tile: no carry crosses a tile boundary
         const int t = threadIdx.x;
@@ -940,7 +940,7 @@ __global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, 
 // zeroing the run before it; a tile that is all ones passes the carry on,
 // which the cross-tile scan already credited to the next tile.  Jobs are the
 // unpack's (product, tile) list, checked 256 at a time (one per thread).
-__global__ void __launch_bounds__(256) k_carry_fix(const DProd* __restrict__ prods, const JobSrc src,
+__global__ void __launch_bounds__(256) k_carry_fix(const DProd* __restrict__ prods, const Job* __restrict__ jobs,
                                                    int64_t njobs) {
     __shared__ unsigned long long first;
     __shared__ int nflag;
@@ -951,14 +951,14 @@ __global__ void __launch_bounds__(256) k_carry_fix(const DProd* __restrict__ pro
         __syncthreads();
         const int64_t ji = j0 + threadIdx.x;
         if (ji < njobs) {
-            const Job jb = job_at(src, ji);
+            const Job jb = jobs[ji];
             const DProd& P = prods[jb.prod];
             if (P.ntl > 1 && (P.agg[jb.tile] & 4u)) flagged[atomicAdd(&nflag, 1)] = ji;
         }
         __syncthreads();
         const int nf = nflag;
         for (int f = 0; f < nf; f++) {
-            const Job jb = job_at(src, flagged[f]);
+            const Job jb = jobs[flagged[f]];
             const DProd& P = prods[jb.prod];
             const int64_t w0 = jb.tile * UNPACK_TL, we = min(w0 + (int64_t)UNPACK_TL, P.rn);
             if (threadIdx.x == 0) first = (unsigned long long)we;
@@ -1059,8 +1059,11 @@ cudaError_t kernels_init(double p1, double p2) {
 
 int kernels_smem_optin() { return g_smem_optin; }
 
-cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& jobs, int64_t njobs,
+cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& src, int64_t njobs,
                         size_t smem, int grid_cap, cudaStream_t st) {
+    // the kernels read an explicit job list (batches expand theirs on the device first)
+    if (src.mode != JM_LIST) return cudaErrorInvalidValue;
+    const Job* jobs = src.list;
     if (njobs <= 0) return cudaSuccess;
     int64_t grid64 = njobs;
     if (kind == JK_FWD || kind == JK_REV) {

@@ -109,7 +109,8 @@ int nbg_batch_launches(const nbg_batch *bt);
 int nbg_batch_destroy(nbg_batch *bt);
 /* Per launch of a batch (up to cap): kernel kind (0 forward pass, 1 last pass
  * with pointwise product, 2 reverse pass, 3 unpack, 4 carry, 5 carries through
- * runs of all-ones limbs, 6 the last pass with one CTA per prime), jobs, and the
+ * runs of all-ones limbs, 6 the last pass with one CTA per prime, 7 the last
+ * pass of products with a kept operand spectrum), jobs, and the
  * algorithmic FP64 instruction count and compulsory bytes of the reference
  * schedule for that launch.  Any output pointer may be NULL. */
 int nbg_batch_stats(const nbg_batch *bt, int32_t *kinds, int64_t *njobs, double *alg_ops, double *alg_bytes,

@@ -728,9 +728,12 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         bmin = std::min(bmin, bch);
         xa_off[(size_t)k] = work;
         work += 2 * (size_t)N;
-        if (P.npass > 1 && !P.sqr) {
+        if (q.keep_b && (P.npass != 1 || P.sqr))
+            return fail(NBG_EINVAL, "product %lld: a kept operand spectrum needs a one-pass product", (long long)k);
+        if ((P.npass > 1 && !P.sqr) || q.keep_b) {
             xb_off[(size_t)k] = work;
             work += 2 * (size_t)N;
+            if (q.keep_b) P.flags |= PF_BSAVE;
         } else {
             xb_off[(size_t)k] = SIZE_MAX;
         }
@@ -790,7 +793,9 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
     std::stable_sort(byclass.begin(), byclass.end(), [&](int32_t x, int32_t y) {
         const int64_t nx = bb.plan_of[(size_t)x]->d.N, ny = bb.plan_of[(size_t)y]->d.N;
         if (nx != ny) return nx > ny;
-        return bb.prods[(size_t)x].plan < bb.prods[(size_t)y].plan;
+        const int px = bb.prods[(size_t)x].plan, py = bb.prods[(size_t)y].plan;
+        if (px != py) return px < py;
+        return (bb.prods[(size_t)x].flags & PF_BSAVE) < (bb.prods[(size_t)y].flags & PF_BSAVE);
     });
     std::vector<int32_t> cls;
     // A batch whose last-pass tiles are fewer than one wave of CTAs (3 per SM)
@@ -804,9 +809,11 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
     const bool split_pwr = pwr_tiles < 3 * (int64_t)std::max(E.num_sms, 1);
     for (size_t i = 0; i < byclass.size();) {
         const int slot = bb.prods[(size_t)byclass[i]].plan;
+        const int keep0 = bb.prods[(size_t)byclass[i]].flags & PF_BSAVE;
         cls.clear();
         double sum_bch = 0;
-        while (i < byclass.size() && bb.prods[(size_t)byclass[i]].plan == slot) {
+        while (i < byclass.size() && bb.prods[(size_t)byclass[i]].plan == slot &&
+               (bb.prods[(size_t)byclass[i]].flags & PF_BSAVE) == keep0) {
             sum_bch += bb.prods[(size_t)byclass[i]].bch;
             cls.push_back(byclass[i++]);
         }
@@ -847,12 +854,13 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
             const DPass& ps = pl.pass[Pn - 1];
             // splitting pays only where a tile set holds more 16-point units
             // than a CTA has threads (smaller tiles just repeat the pack)
-            const bool split = split_pwr && (int64_t)ps.G * ps.C * 2 * nop > 16 * PASS_THREADS;
+            const bool keep = keep0 != 0;
+            const bool split = !keep && split_pwr && (int64_t)ps.G * ps.C * 2 * nop > 16 * PASS_THREADS;
             const size_t smem = sizeof(double) * (P0.sqr ? 1 : 2) * (split ? 1 : 2) *
                                 (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
             const double jobs = (double)ps.ntiles * nc;  // tiles of both primes (the work, split or not)
-            Group& g = group_of(pmax - 1, split ? JK_PWR_SPLIT : JK_PWR, smem);
+            Group& g = group_of(pmax - 1, keep ? JK_PWR_KEEP : split ? JK_PWR_SPLIT : JK_PWR, smem);
             emit(g, ps, split ? 2 : 1, (Pn - 1) << 8);  // split: "operand" is the prime
             g.ops += jobs * 2.0 * (nop * pass_ops(pl, ps, true) + 7.0 * pts + pass_ops(pl, ps, false));
             const double in_b = Pn == 1 ? (double)ps.ntiles * nop * pts * sum_bch / 8.0 : jobs * 2.0 * nop * 8.0 * pts;

@@ -96,6 +96,8 @@ struct ProdIn {
     int64_t m, n;
     int64_t bits_a, bits_b;
     int sqr;
+    // one-pass products only: keep operand b's spectrum in workspace (PF_BSAVE)
+    int keep_b = 0;
 };
 
 struct Launch {

@@ -273,6 +273,8 @@ struct FuseTiles {
     int sq;
     int G, lc, Qb, j0;
     int pfix;  // -1: tiles of both primes; 0 or 1: only that prime's (a, b) tiles
+    int bspec; // b's tiles hold its spectrum already: its forward round is skipped
+    int bsave; // b's spectrum is stored after this round: write its forward result back
 };
 
 __device__ __forceinline__ void pw4(double* a, const double* b, Fp F) {
@@ -335,7 +337,7 @@ __device__ NBG_ROUND void fused_r16(const FuseTiles& T, const DStage& A, const D
         const int stepA = q16 * T.Qb;
         const double wB[4] = {0.0, __ldg(twB), __ldg(twB + QB), __ldg(twB + 2 * QB)};
         double va[16];
-        if (!T.sq) {
+        if (!T.sq && !T.bspec) {
             // b's forward round goes back to its own shared slots (same thread),
             // keeping one operand in registers at a time
 #pragma unroll
@@ -386,7 +388,7 @@ __device__ NBG_ROUND void fused_r8(const FuseTiles& T, const DStage& A) {
         }
 #pragma unroll
         for (int op = 0; op < 2; op++) {
-            if (op == 1 && T.sq) break;
+            if (op == 1 && (T.sq || T.bspec)) break;
             double* v = op ? vb : va;
             double y[4] = {v[0], v[2], v[4], v[6]};
             butterfly<4, true>(y, w0, &wi, F);
@@ -396,6 +398,10 @@ __device__ NBG_ROUND void fused_r8(const FuseTiles& T, const DStage& A) {
             v[1] = z[0]; v[3] = z[1]; v[5] = z[2]; v[7] = z[3];
 #pragma unroll
             for (int i = 0; i < 4; i++) butterfly2(v[2 * i], v[2 * i + 1], F);
+        }
+        if (T.bsave) {  // b's forward result lives in registers here: the stored spectrum needs it
+#pragma unroll
+            for (int k = 0; k < 8; k++) sb[sp(8 * b + k)] = vb[k];
         }
 #pragma unroll
         for (int k = 0; k < 2; k++) pw4(va + 4 * k, T.sq ? va + 4 * k : vb + 4 * k, F);
@@ -584,7 +590,10 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restr
 
 // Last pass, both primes: forward on a (and b), pointwise, reverse on a.
 // Tiles: products [a0, b0, a1, b1], squares [a0, a1].
-template <bool SPLIT>
+// SPLIT: one CTA per prime (JK_PWR_SPLIT).  KEEPB: launches of products with
+// a kept operand spectrum (JK_PWR_KEEP; PF_BSAVE / PF_BSPEC), compiled apart
+// so the other launches carry none of that code.
+template <bool SPLIT, bool KEEPB>
 __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const Job* __restrict__ jobs, int64_t njobs) {
@@ -609,10 +618,19 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
         double* b1 = sq ? a1 : smem + 3 * stride;
         const int p0 = pf >= 0 ? pf : 0;
         const int cnt = ps.G * ps.C;
+        // operand b's spectrum: kept from an earlier run (bspec) or to be kept (bsave)
+        const bool bspec = KEEPB && !sq && (P.flags & PF_BSPEC);
+        const bool bsave = KEEPB && !sq && (P.flags & PF_BSAVE);
         __syncthreads();
         if (pass == 0 && !(P.flags & PF_PRELOADED)) {
             pack_tile2(a0, pf >= 0 ? a0 : a1, P.a, P.m, P.bch, P.nca, ps, base);
-            if (!sq) pack_tile2(b0, pf >= 0 ? b0 : b1, P.b, P.n, P.bch, P.ncb, ps, base);
+            if (bspec) {
+                load_tile_async(b0, P.xb[p0], ps, base);
+                if (pf < 0) load_tile_async(b1, P.xb[1], ps, base);
+                cp_async_wait_all();
+            } else if (!sq) {
+                pack_tile2(b0, pf >= 0 ? b0 : b1, P.b, P.n, P.bch, P.ncb, ps, base);
+            }
         } else {
             load_tile_async(a0, P.xa[p0], ps, base);
             if (!sq) load_tile_async(b0, P.xb[p0], ps, base);
@@ -624,6 +642,8 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
         }
         Tiles TF = pf < 0 ? make_tiles(smem, stride, sq ? 2 : 4, sq ? 0 : 1, ps, j0)
                           : make_tiles(smem, stride, sq ? 1 : 2, 30, ps, j0);
+        if (bspec)  // b is transformed already: the forward rounds run on the a tiles only
+            TF = pf < 0 ? make_tiles(a0, (int)(a1 - a0), 2, 0, ps, j0) : make_tiles(a0, stride, 1, 30, ps, j0);
         Tiles TR = pf < 0 ? make_tiles(a0, (int)(a1 - a0), 2, 0, ps, j0) : make_tiles(a0, stride, 1, 30, ps, j0);
         TF.pfix = pf;
         TR.pfix = pf;
@@ -642,13 +662,24 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
             FT.Qb = (int)ps.Qb;
             FT.j0 = j0;
             FT.pfix = pf;
+            FT.bspec = bspec;
+            FT.bsave = bsave;
             const int s0 = ps.rstage[nr - 1];
             if (lastk == RK_R16) fused_r16(FT, pl.st[s0], pl.st[s0 + 1]);
             else fused_r8(FT, pl.st[s0]);
+            if (bsave) {  // b's tiles are fully transformed now; the reverse leaves them alone
+                __syncthreads();
+                store_tile(b0, P.xb[p0], ps, base);
+                if (pf < 0) store_tile(b1, P.xb[1], ps, base);
+            }
             for (int r = nr - 2; r >= 0; r--) run_round<false>(TR, pl, ps.rkind[r], ps.rstage[r]);
             __syncthreads();
         } else {
             run_pass<true>(TF, pl, ps);
+            if (bsave) {
+                store_tile(b0, P.xb[p0], ps, base);
+                if (pf < 0) store_tile(b1, P.xb[1], ps, base);
+            }
             if (pf < 0) {
                 const Fp F0 = fpctx(0), F1 = fpctx(1);
                 for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
@@ -1043,7 +1074,8 @@ cudaError_t kernels_init(double p1, double p2) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const void* ks[] = {(const void*)k_fwd<3>, (const void*)k_fwd<4>, (const void*)k_pwr<false>, (const void*)k_pwr<true>,
+    const void* ks[] = {(const void*)k_fwd<3>, (const void*)k_fwd<4>, (const void*)k_pwr<false, false>, (const void*)k_pwr<true, false>,
+                        (const void*)k_pwr<false, true>,
                         (const void*)k_rev<3>, (const void*)k_rev<4>, (const void*)k_unpack};
     for (const void* k : ks) {
         cudaFuncAttributes fa;
@@ -1079,8 +1111,9 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
             if (smem <= COL4_MAX_SMEM) k_fwd<4><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
             else k_fwd<3><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
             break;
-        case JK_PWR: k_pwr<false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
-        case JK_PWR_SPLIT: k_pwr<true><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_PWR: k_pwr<false, false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_PWR_SPLIT: k_pwr<true, false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_PWR_KEEP: k_pwr<false, true><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
         case JK_REV:
             if (smem <= COL4_MAX_SMEM) k_rev<4><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
             else k_rev<3><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);

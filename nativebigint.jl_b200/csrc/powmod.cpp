@@ -187,6 +187,16 @@ struct PmGraph {
     }
 };
 
+// Whether a product of these magnitudes runs as one pass (its operand b's
+// spectrum can then be kept between runs).
+static bool one_pass(Engine& E, int64_t bits_a, int64_t bits_b) {
+    int b = 0;
+    int64_t N = 0;
+    PlanRec* pr = nullptr;
+    if (ntt_params(bits_a, bits_b, &b, &N) != NBG_OK || E.get_plan(N, 0, &pr) != NBG_OK) return false;
+    return pr->d.npass == 1;
+}
+
 // Steps replayed per graph launch.
 constexpr int64_t PM_GRAPH_STEPS = 64;
 
@@ -288,8 +298,12 @@ static int powmod_run(Engine& E, const nbg_powmod_desc* d, int64_t count, int64_
         uint64_t* q2 = d_q2 + c * q2_stride;
         const int64_t l = lmu[(size_t)c];
         in1[(size_t)c] = ProdIn{sl + (int64_t)S.acc() * k, sl + (int64_t)S.one() * k, T, k, k, 64 * k, 64 * k, 0};
+        // mu and m are the same on every step: as operand b their transforms
+        // are kept from the first run (one-pass products) and reused
         in2[(size_t)c] = ProdIn{T + (k - 1), d_mu + c * lmu_max, q2, k + 1, l, 64 * (k + 1), bits_mu[(size_t)c], 0};
-        in3[(size_t)c] = ProdIn{d_mod + c * k, q2 + (k + 1), d_r2 + c * C.r2_stride, k, l, bits_m[(size_t)c], 64 * l, 0};
+        in3[(size_t)c] = ProdIn{q2 + (k + 1), d_mod + c * k, d_r2 + c * C.r2_stride, l, k, 64 * l, bits_m[(size_t)c], 0};
+        in2[(size_t)c].keep_b = one_pass(E, 64 * (k + 1), bits_mu[(size_t)c]);
+        in3[(size_t)c].keep_b = one_pass(E, 64 * l, bits_m[(size_t)c]);
     }
     BatchBuild bb[3];
     char* reg[3];
@@ -302,6 +316,22 @@ static int powmod_run(Engine& E, const nbg_powmod_desc* d, int64_t count, int64_
     }
     C.prods = (DProd*)(reg[0] + bb[0].off_prods);
     PM_TRY(pm_launch_init(C, d_bases, d_lb, st));
+    // one run of the q1*mu and q3*m batches stores mu's and m's spectra
+    // (PF_BSAVE; their other inputs are zero or already defined here), then
+    // every later run loads them (PF_BSPEC)
+    for (int i = 1; i < 3; i++) {
+        if ((rc = run_launches(E, bb[i], reg[i], st, false))) return rc;
+        bool any = false;
+        for (DProd& P : bb[i].prods)
+            if (P.flags & PF_BSAVE) {
+                P.flags = (P.flags & ~PF_BSAVE) | PF_BSPEC;
+                any = true;
+            }
+        if (any)
+            PM_TRY(cudaMemcpyAsync(reg[i] + bb[i].off_prods, bb[i].prods.data(), sizeof(DProd) * bb[i].prods.size(),
+                                   cudaMemcpyHostToDevice, st));
+    }
+    PM_TRY(cudaStreamSynchronize(st));  // the host copies above read bb[i].prods
     // one graph of PM_GRAPH_STEPS steps, replayed until every chain is done
     const int64_t G = std::min(PM_GRAPH_STEPS, max_steps);
     PmGraph gr;

@@ -180,6 +180,7 @@ enum JobKind : int32_t {
     JK_CARRY = 4, // cross-tile carry scan and fix-up (one job per product)
     JK_CARRYFIX = 5, // carries through runs of all-ones limbs (one job per unpack tile)
     JK_PWR_SPLIT = 6,// JK_PWR with one job per prime (sub bit 1) for small batches
+    JK_PWR_KEEP = 7, // JK_PWR for products with a kept operand spectrum (PF_BSAVE / PF_BSPEC)
 };
 
 constexpr int UNPACK_TL = 1024;  // output limbs per unpack tile
@@ -192,5 +193,11 @@ NBG_HD inline int tile_stride_doubles(int n) { return ((n + (n >> 4) + 1) + 1) &
 
 // DProd.flags
 constexpr int32_t PF_PRELOADED = 1;  // pass 0 loads xa/xb as-is instead of packing limbs
+// One-pass products whose operand b is the same on every run (a modulus or a
+// reciprocal in the powermod chains): a run with PF_BSAVE stores b's forward
+// transform (both primes) in xb; runs with PF_BSPEC load it from there instead
+// of packing and transforming b again.
+constexpr int32_t PF_BSAVE = 2;
+constexpr int32_t PF_BSPEC = 4;
 
 }  // namespace nbg

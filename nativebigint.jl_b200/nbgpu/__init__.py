@@ -319,7 +319,7 @@ class Batch:
         ops = (ctypes.c_double * n)()
         byt = (ctypes.c_double * n)()
         _check(lib().nbg_batch_stats(self._h, kinds, njobs, ops, byt, n))
-        names = {0: "k_fwd", 1: "k_pwr", 2: "k_rev", 3: "k_unpack", 4: "k_carry", 5: "k_carry_fix", 6: "k_pwr"}
+        names = {0: "k_fwd", 1: "k_pwr", 2: "k_rev", 3: "k_unpack", 4: "k_carry", 5: "k_carry_fix", 6: "k_pwr", 7: "k_pwr"}
         return [dict(kind=names[kinds[i]], jobs=njobs[i], alg_ops=ops[i], alg_bytes=byt[i]) for i in range(n)]
 
     def profile(self, stream=None) -> list[float]:

@@ -105,6 +105,44 @@ function gpu_mul_batch!(descs::Vector{NbgDesc})
     return nothing
 end
 
+# Many powermod(b, e, m) calls with moduli of one size k (powermod_limbs on its
+# Barrett branch, src/algorithms.jl:17-107): each chain's r gets b^e mod m
+# (k limbs); b has at most k limbs, e is nonzero, m[k] != 0 and m > 1.
+struct NbgPowmodDesc
+    r::Ptr{Limb}
+    b::Ptr{Limb}
+    e::Ptr{Limb}
+    m::Ptr{Limb}
+    lb::Int64
+    le::Int64
+end
+
+function gpu_powermod_batch!(rs::Vector{Memory{Limb}}, bs::Vector{Memory{Limb}}, es::Vector{Memory{Limb}},
+                             ms::Vector{Memory{Limb}}, k::Int)
+    n = length(ms)
+    (length(rs) == n && length(bs) == n && length(es) == n) || throw(ArgumentError("one r, b, e per modulus"))
+    GC.@preserve rs bs es ms begin
+        descs = [NbgPowmodDesc(pointer(rs[i]), pointer(bs[i]), pointer(es[i]), pointer(ms[i]),
+                               length(bs[i]), length(es[i])) for i in 1:n]
+        rc = ccall((:nbg_powermod_batch, LIB), Cint, (Ptr{NbgPowmodDesc}, Int64, Int64), descs, n, k)
+    end
+    check(rc)
+    return nothing
+end
+
+# Limbs of the value of little-endian base-bb chunks (radix_combine,
+# src/nbig.jl:410-417): NBig parsing above its divide-and-conquer threshold.
+function gpu_radix_combine(chunks::Vector{Limb}, bb::Limb)
+    out = Memory{Limb}(undef, max(length(chunks), 1))
+    len = Ref{Int64}(0)
+    GC.@preserve out chunks begin
+        rc = ccall((:nbg_radix_combine, LIB), Cint, (Ptr{Limb}, Int64, Ptr{Limb}, Int64, UInt64, Ref{Int64}),
+                   pointer(out), length(out), pointer(chunks), length(chunks), bb, len)
+    end
+    check(rc)
+    return out, Int(len[])
+end
+
 # Replaces the engine entry points of the enclosing NativeBigInt module so every
 # NTT-sized mul!/sqr!/mul_bal! (src/mul.jl:134, :146, :161, :388-390) and NBig *
 # (src/nbig.jl:124-140) run on the GPU.

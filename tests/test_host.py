@@ -299,3 +299,19 @@ def test_odd_multiplier_landings():
                  (1439744, 315 * 2**14), (10928128, 315 * 2**17)):
         assert O.ntt_params(64 * n, 64 * n)[1] == N
         assert nbgpu.ntt_params(64 * n, 64 * n)[1] == N
+
+
+def test_column_major_tile_order_is_a_permutation():
+    """Column passes visit tile t_lin = jc * nblk + blk as tile blk * per + jc
+    (job segments, types.h job_at): every tile once, and runs of consecutive
+    visits share the column jc (hence the twiddle columns)."""
+    rng = np.random.default_rng(3)
+    for _ in range(50):
+        per = int(rng.integers(2, 300))
+        nblk = int(rng.integers(2, 300))
+        n = per * nblk
+        seen = [(t % nblk) * per + t // nblk for t in range(n)]
+        assert sorted(seen) == list(range(n))
+        # within a run of nblk consecutive visits the column index is fixed
+        for t0 in range(0, n, nblk):
+            assert len({seen[t] % per for t in range(t0, t0 + nblk)}) == 1

@@ -191,40 +191,53 @@ int host_batch(const nbg_desc* descs, int64_t count) {
             rc = fail(NBG_ENOMEM, "device region of %zu bytes unavailable", c.region);
             break;
         }
-        size_t ii = 0;
-        for (int64_t k = 0; k < c.count; k++) {
-            const ProdIn& q = in[(size_t)(c.start + k)];
-            DProd& P = c.bb.prods[(size_t)k];
-            P.a = (const uint64_t*)(base + base_in + ioff[ii++]);
-            P.b = q.sqr ? P.a : (const uint64_t*)(base + base_in + ioff[ii++]);
-            P.r = (uint64_t*)(base + base_out + ooff[(size_t)k]);
-        }
-        // descriptors and job table through the slot's pinned staging buffer
-        if ((rc = E.ensure_stage(buf, c.bb.head_bytes))) break;
-        bind_batch(c.bb, base);
-        stage_batch(c.bb, E.stage[buf]);
-        if (cudaMemcpyAsync(base, E.stage[buf], c.bb.head_bytes, cudaMemcpyHostToDevice, E.copy_in) != cudaSuccess) {
-            rc = fail(NBG_ECUDA, "descriptor copy failed");
+        // everything after the allocation: on an error the region is freed
+        // once the streams are idle
+        int crc = NBG_OK;
+        do {
+            size_t ii = 0;
+            for (int64_t k = 0; k < c.count; k++) {
+                const ProdIn& q = in[(size_t)(c.start + k)];
+                DProd& P = c.bb.prods[(size_t)k];
+                P.a = (const uint64_t*)(base + base_in + ioff[ii++]);
+                P.b = q.sqr ? P.a : (const uint64_t*)(base + base_in + ioff[ii++]);
+                P.r = (uint64_t*)(base + base_out + ooff[(size_t)k]);
+            }
+            // descriptors and job table through the slot's pinned staging buffer
+            if ((crc = E.ensure_stage(buf, c.bb.head_bytes))) break;
+            bind_batch(c.bb, base);
+            stage_batch(c.bb, E.stage[buf]);
+            if (cudaMemcpyAsync(base, E.stage[buf], c.bb.head_bytes, cudaMemcpyHostToDevice, E.copy_in) != cudaSuccess) {
+                crc = fail(NBG_ECUDA, "descriptor copy failed");
+                break;
+            }
+            for (const Span& sp : c.in_spans)
+                if (cudaMemcpyAsync(base + base_in + sp.d, sp.h, sp.n, cudaMemcpyHostToDevice, E.copy_in) != cudaSuccess) {
+                    crc = fail(NBG_ECUDA, "operand copy failed");
+                    break;
+                }
+            if (crc) break;
+            cudaEventRecord(ev_in[buf], E.copy_in);
+            cudaStreamWaitEvent(E.stream, ev_in[buf], 0);
+            if ((crc = run_launches(E, c.bb, base, E.stream))) break;
+            cudaEventRecord(ev_comp[buf], E.stream);
+            cudaStreamWaitEvent(E.copy_out, ev_comp[buf], 0);
+            for (const Span& sp : c.out_spans)
+                if (cudaMemcpyAsync((void*)sp.h, base + base_out + sp.d, sp.n, cudaMemcpyDeviceToHost, E.copy_out) !=
+                    cudaSuccess) {
+                    crc = fail(NBG_ECUDA, "result copy failed");
+                    break;
+                }
+            if (crc) break;
+        } while (0);
+        if (crc) {
+            cudaStreamSynchronize(E.copy_in);
+            cudaStreamSynchronize(E.stream);
+            cudaStreamSynchronize(E.copy_out);
+            cudaFreeAsync(base, E.copy_out);
+            rc = crc;
             break;
         }
-        for (const Span& sp : c.in_spans)
-            if (cudaMemcpyAsync(base + base_in + sp.d, sp.h, sp.n, cudaMemcpyHostToDevice, E.copy_in) != cudaSuccess) {
-                rc = fail(NBG_ECUDA, "operand copy failed");
-                break;
-            }
-        if (rc) break;
-        cudaEventRecord(ev_in[buf], E.copy_in);
-        cudaStreamWaitEvent(E.stream, ev_in[buf], 0);
-        if ((rc = run_launches(E, c.bb, base, E.stream))) break;
-        cudaEventRecord(ev_comp[buf], E.stream);
-        cudaStreamWaitEvent(E.copy_out, ev_comp[buf], 0);
-        for (const Span& sp : c.out_spans)
-            if (cudaMemcpyAsync((void*)sp.h, base + base_out + sp.d, sp.n, cudaMemcpyDeviceToHost, E.copy_out) !=
-                cudaSuccess) {
-                rc = fail(NBG_ECUDA, "result copy failed");
-                break;
-            }
-        if (rc) break;
         cudaFreeAsync(base, E.copy_out);
         cudaEventRecord(ev_out[buf], E.copy_out);
     }

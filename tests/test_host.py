@@ -315,3 +315,31 @@ def test_column_major_tile_order_is_a_permutation():
         # within a run of nblk consecutive visits the column index is fixed
         for t0 in range(0, n, nblk):
             assert len({seen[t] % per for t in range(t0, t0 + nblk)}) == 1
+
+
+def test_argument_errors_of_the_caller_entry_points():
+    """The powermod, radix, low-half and sum-of-products entry points reject bad
+    arguments before they touch a device."""
+    L = nbgpu.lib()
+    one = np.ones(4, dtype=np.uint64)
+    r = np.zeros(4, dtype=np.uint64)
+    # powermod: base longer than the modulus, zero-length exponent
+    d = (nbgpu.PowmodDesc * 1)()
+    d[0] = nbgpu.PowmodDesc(r.ctypes.data, one.ctypes.data, one.ctypes.data, one.ctypes.data, 3, 1)
+    assert L.nbg_powermod_batch(ctypes.cast(d, ctypes.c_void_p), 1, 2) == nbgpu.NBG_EINVAL
+    d[0] = nbgpu.PowmodDesc(r.ctypes.data, one.ctypes.data, one.ctypes.data, one.ctypes.data, 1, 0)
+    assert L.nbg_powermod_batch(ctypes.cast(d, ctypes.c_void_p), 1, 2) == nbgpu.NBG_EINVAL
+    assert L.nbg_powermod_batch(None, 1, 2) == nbgpu.NBG_EINVAL
+    # radix combine: a chunk not below the base, too small an output
+    ln = ctypes.c_int64()
+    c = np.array([3, 10], dtype=np.uint64)
+    assert L.nbg_radix_combine(r.ctypes.data, 4, c.ctypes.data, 2, 10, ctypes.byref(ln)) == nbgpu.NBG_EINVAL
+    assert L.nbg_radix_combine(r.ctypes.data, 1, c.ctypes.data, 2, 100, ctypes.byref(ln)) == nbgpu.NBG_EINVAL
+    assert L.nbg_radix_combine(r.ctypes.data, 4, c.ctypes.data, 2, 1, ctypes.byref(ln)) == nbgpu.NBG_EINVAL
+    # sums of products: r too short, null matrix entries
+    assert L.nbg_mul2add_dev(r.ctypes.data, 3, one.ctypes.data, 2, one.ctypes.data, 2, one.ctypes.data, 1,
+                             one.ctypes.data, 1, None) == nbgpu.NBG_EINVAL
+    m4 = (ctypes.c_void_p * 4)(None, None, None, None)
+    assert L.nbg_matrix22_mul_dev(m4, 1, m4, 1, None) == nbgpu.NBG_EINVAL
+    # low halves: null operand, k < 1
+    assert L.nbg_mullo(r.ctypes.data, one.ctypes.data, 2, None, 2, 2) == nbgpu.NBG_EINVAL

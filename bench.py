@@ -45,43 +45,9 @@ WORKLOAD = "10,000 mixed products: larger operand log-uniform [152, 65536] limbs
 
 
 # ---------------------------------------------------------------------------
-# workload
+# workload (the seeded generator lives in the package: nbgpu/workload.py)
 
-def gen_workload(seed: int, count: int, shape: tuple[int, int] | None = None, square: bool = False):
-    """The mixed 10,000-product batch; or, with `shape`, `count` copies of one
-    m x n shape (all squares with `square`), for per-class profiling."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    if shape:
-        m = np.full(count, shape[0], dtype=np.int64)
-        n = np.full(count, shape[1], dtype=np.int64)
-        sq = np.full(count, bool(square))
-    else:
-        m = np.exp(rng.uniform(math.log(152), math.log(65536), count)).astype(np.int64)
-        ratio = rng.uniform(0.25, 1.0, count)
-        n = np.maximum(1, np.round(m * ratio).astype(np.int64))
-        sq = rng.random(count) < 0.2
-    n = np.where(sq, m, n)
-    # operand limbs, one flat array: a_k then (for products) b_k
-    la = m.copy()
-    lb = np.where(sq, 0, n)
-    off_a = np.zeros(count, dtype=np.int64)
-    off_b = np.zeros(count, dtype=np.int64)
-    pos = 0
-    for k in range(count):
-        off_a[k] = pos
-        pos += int(la[k])
-        off_b[k] = pos
-        pos += int(lb[k])
-    limbs = rng.integers(0, 2**64, pos, dtype=np.uint64, endpoint=False)
-    for top in (off_a + la - 1, (off_b + lb - 1)[~sq]):  # top limbs nonzero
-        limbs[top] = np.where(limbs[top] == 0, np.uint64(1), limbs[top])
-    out_off = np.concatenate([[0], np.cumsum(m + n)[:-1]]).astype(np.int64)
-    return dict(m=m, n=n, sq=sq, off_a=off_a, off_b=off_b, limbs=limbs, out_off=out_off,
-                out_total=int((m + n).sum()))
-
-
-def bits_of(limbs: np.ndarray, off: int, ln: int) -> int:
-    return 64 * (ln - 1) + int(limbs[off + ln - 1]).bit_length()
+from nbgpu.workload import bits_of, gen_workload  # noqa: E402
 
 
 # ---------------------------------------------------------------------------
@@ -237,6 +203,22 @@ def fp64_peak() -> dict:
     return {"dfma_per_s": fma.value, "dadd_per_s": add.value}
 
 
+def hbm_peak() -> tuple[float, str]:
+    """HBM copy bandwidth for the byte roofline: MEASURED_PEAKS.json's hbm_gbs
+    when that file is present, else the pool's earlier measured fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        v = d.get("hbm_gbs")
+        if isinstance(v, dict):
+            v = v.get("value")
+        if v:
+            return float(v), "measured: MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, ValueError, AttributeError):
+        pass
+    return 6650.0, "fallback: 6.65 TB/s (MEASURED_PEAKS.json absent)"
+
+
 def traffic_from_profiles(kernel: str, point_primes: float):
     """DRAM bytes of `kernel` for one batch: the committed ncu measurement of
     bytes per transform point per prime (profiles/ncu_traffic.json, taken on
@@ -345,6 +327,7 @@ def run_ours(args, rank: int, world: int) -> None:
         dom = max(kern, key=lambda k: kern[k]["ms"])
         D = kern[dom]
         peak = fp64_peak()
+        hbm_gbs, hbm_src = hbm_peak()
         achieved = D["ops"] / (D["ms"] / 1e3) / 1e12
         pk = peak["dfma_per_s"] / 1e12
         tot_ops = sum(st_["alg_ops"] for st_ in stats)
@@ -356,8 +339,8 @@ def run_ours(args, rank: int, world: int) -> None:
             "alg_ops": D["ops"], "ms": D["ms"], "launches": D["launches"],
             "traffic_source": "profiles/ncu_traffic.json bytes per point per prime x this batch's points",
             "hbm": {"alg_bytes": D["bytes"],
-                    "achieved_gbs": D["bytes"] / (D["ms"] / 1e3) / 1e9, "peak_gbs": 6542.7,
-                    "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+                    "achieved_gbs": D["bytes"] / (D["ms"] / 1e3) / 1e9, "peak_gbs": hbm_gbs,
+                    "peak_source": hbm_src},
             "kernels": {k: {"ms_per_step": v["ms"], "share": v["ms"] / sum(x["ms"] for x in kern.values()),
                             "alg_tops": v["ops"] / (v["ms"] / 1e3) / 1e12 if v["ms"] else 0.0}
                         for k, v in kern.items()},

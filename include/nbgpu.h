@@ -7,7 +7,9 @@
  * only; limbs are little-endian uint64_t.  All entry points return an int
  * status (NBG_OK = 0) and never abort; nbg_last_error() describes the last
  * failure on the calling thread.  The library is thread-safe: calls on one
- * device are serialized by an internal lock.
+ * device are serialized by an internal lock.  It keeps device state (plans,
+ * twiddle tables, workspace, kernel settings) for the life of the process, so
+ * it must not outlive a cudaDeviceReset of a device it has used.
  */
 #ifndef NBGPU_H
 #define NBGPU_H
@@ -63,7 +65,9 @@ int nbg_sqr_dev(uint64_t *r, const uint64_t *a, int64_t n, void *stream);
  * fixed 16 MiB device array inside the library (held on every GPU that loads
  * the library until exit), located once per device with cudaGetSymbolAddress
  * on the first call there — make that first call before any stream capture.
- * Products that do not fit return NBG_ENOMEM: transform lengths above about
+ * Every call synchronizes `stream`: it reads the operands' top limbs to the
+ * host to size the transform (twice more when it builds twiddle tables for a
+ * new transform length).  Products that do not fit return NBG_ENOMEM: transform lengths above about
  * 3.4e5 points for products (balanced operands above about 2^16 limbs) or
  * 5.2e5 points for squares.  All calls
  * share the array: calls that overlap on the GPU race; order them on one
@@ -127,15 +131,19 @@ int nbg_batch_profile(nbg_batch *bt, void *stream, float *ms, int32_t cap);
  * the next one from everything pending that fits in the free arena.
  * A new batch starts at once while fewer than two batches are in flight;
  * with two or more it starts when the pending requests hold at least
- * batch_points transform points (0: 2^23), so that under load batches stay
+ * batch_points transform points (0: 2^23), or when the oldest pending request
+ * has waited max_hold_us (0: 2000 us), so that under load batches stay
  * large enough to fill the GPU while an idle GPU still takes a lone request
- * immediately.  max_batch bounds a batch (0: no bound); max_queue bounds
- * pending requests (0: no bound; past it nbg_submit returns NBG_EBUSY). */
+ * immediately and no request waits on the point threshold for long.
+ * max_batch bounds a batch (0: no bound); max_queue bounds
+ * pending requests (0: no bound; past it nbg_submit returns NBG_EBUSY).
+ * Requests whose result overlaps an operand fail with NBG_EINVAL. */
 typedef struct nbg_server_opts {
     int64_t hbm_budget_bytes;
     int64_t max_batch;
     int64_t max_queue;
     int64_t batch_points;
+    int64_t max_hold_us;
 } nbg_server_opts;
 
 typedef struct nbg_server_stats_t {
@@ -289,6 +297,11 @@ const char *nbg_last_error(void);
 void *nbg_default_stream(void);
 /* counters: kernel launches issued by this library since load */
 int64_t nbg_launch_count(void);
+/* Diagnostic, no counterpart in the reference: the binary version (major * 10
+ * + minor, cudaFuncGetAttributes) of the transform kernels as the CUDA runtime
+ * loaded them on the current device, 100 for the sm_100a build; NBG_ECUDA
+ * when the device cannot run them. */
+int nbg_kernel_arch(int32_t *version);
 
 #ifdef __cplusplus
 }

@@ -483,6 +483,15 @@ void* nbg_default_stream(void) {
 
 int64_t nbg_launch_count(void) { return g_launches.load(); }
 
+int nbg_kernel_arch(int32_t* version) {
+    if (!version) return fail(NBG_EINVAL, "null pointer");
+    int v = 0;
+    cudaError_t e = kernels_binary_version(&v);
+    if (e != cudaSuccess) return fail(NBG_ECUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
+    *version = v;
+    return NBG_OK;
+}
+
 int nbg_mul(uint64_t* r, const uint64_t* a, int64_t m, const uint64_t* b, int64_t n) {
     if (!b) return fail(NBG_EINVAL, "null pointer");
     API_LOCK();

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "butterfly.cuh"
 #include "kernels.h"
@@ -1050,7 +1051,9 @@ __global__ void k_twiddle(double* __restrict__ out, int m, int64_t Q, int64_t st
 // ---------------------------------------------------------------------------
 // Host-side launch helpers
 
-static int g_smem_optin = 0;
+// Written once per kernels_init with its final value, so a concurrent reader
+// never sees a partial result.
+static std::atomic<int> g_smem_optin{0};
 
 cudaError_t kernels_init(double p1, double p2) {
     Fp h[2] = {{p1, 1.0 / p1}, {p2, 1.0 / p2}};
@@ -1071,9 +1074,9 @@ cudaError_t kernels_init(double p1, double p2) {
     g[1] = g[0] / p2;
     e = cudaMemcpyToSymbol(c_garner, g, sizeof g);
     if (e != cudaSuccess) return e;
-    int dev = 0;
+    int dev = 0, optin = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const void* ks[] = {(const void*)k_fwd<3>, (const void*)k_fwd<4>, (const void*)k_pwr<false, false>, (const void*)k_pwr<true, false>,
                         (const void*)k_pwr<false, true>,
                         (const void*)k_rev<3>, (const void*)k_rev<4>, (const void*)k_unpack};
@@ -1081,15 +1084,22 @@ cudaError_t kernels_init(double p1, double p2) {
         cudaFuncAttributes fa;
         e = cudaFuncGetAttributes(&fa, k);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 g_smem_optin - (int)fa.sharedSizeBytes);
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
         if (e != cudaSuccess) return e;
     }
-    g_smem_optin -= 4096;  // headroom for the largest static allocation (k_unpack)
+    g_smem_optin.store(optin - 4096);  // headroom for the largest static allocation (k_unpack)
     return cudaSuccess;
 }
 
-int kernels_smem_optin() { return g_smem_optin; }
+int kernels_smem_optin() { return g_smem_optin.load(); }
+
+cudaError_t kernels_binary_version(int* version) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)k_pwr<false, false>);
+    if (e != cudaSuccess) return e;
+    *version = fa.binaryVersion;
+    return cudaSuccess;
+}
 
 cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& src, int64_t njobs,
                         size_t smem, int grid_cap, cudaStream_t st) {

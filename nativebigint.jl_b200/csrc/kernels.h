@@ -9,6 +9,8 @@ namespace nbg {
 // Uploads the prime constants and raises the kernels' dynamic shared-memory cap.
 cudaError_t kernels_init(double p1, double p2);
 int kernels_smem_optin();
+// binaryVersion of the pass kernels as loaded on the current device
+cudaError_t kernels_binary_version(int* version);
 
 // An explicit job list as a launch's job source.
 inline JobSrc job_list(const Job* l) {

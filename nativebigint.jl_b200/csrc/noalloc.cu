@@ -24,7 +24,13 @@
 // address: the set-up below asks the runtime for the real address with
 // cudaGetSymbolAddress, once per device, with that device current, on the
 // first call made on the device.  Make that first call before any stream
-// capture begins.
+// capture begins.  The address and the kernels' settings are kept for the
+// life of the process, so the library must not outlive a cudaDeviceReset of
+// a device it has used.
+//
+// Every call waits for its stream once: it copies the operands' top limbs to
+// the host to size the transform (fp_ntt_params needs their magnitude bits),
+// and a call that builds new twiddle tables waits once more per prime.
 //
 // All calls share the one array and it keeps the last call's contents: the
 // twiddle tables of the last transform length are reused when the next call

@@ -40,6 +40,7 @@ namespace {
 constexpr int MAX_FLIGHT = 3;
 constexpr int NSIDE = 3;                     // side streams per slot: a step's launches run side by side
 constexpr int64_t DEFAULT_BATCH_POINTS = int64_t(1) << 23;
+constexpr int64_t DEFAULT_MAX_HOLD_US = 2000;
 
 double now_us() {
     return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -143,6 +144,7 @@ struct nbg_server {
     bool wake = false;  // a submission or a batch completion since the worker last looked
     double limbs_done = 0, t_first = 0, t_last = 0;
 
+    double hold_us() const { return (double)(opts.max_hold_us > 0 ? opts.max_hold_us : DEFAULT_MAX_HOLD_US); }
     void run();
     bool launch_batch(std::unique_lock<std::mutex>& lk);
     void retire(std::unique_lock<std::mutex>& lk);
@@ -171,7 +173,9 @@ void nbg_server::fail_front(int rc) {
 bool nbg_server::launch_batch(std::unique_lock<std::mutex>& lk) {
     if (pending.empty() || (int)flights.size() >= MAX_FLIGHT) return false;
     const double target = (double)(opts.batch_points > 0 ? opts.batch_points : DEFAULT_BATCH_POINTS);
-    if (flights.size() >= 2 && pending_points < target) return false;  // let the next batch grow
+    // let the next batch grow, unless its oldest request has waited max_hold_us
+    if (flights.size() >= 2 && pending_points < target && now_us() - reqs[pending.front()].t_submit < hold_us())
+        return false;
     std::vector<int64_t> ids;
     std::vector<ProdIn> in;
     std::vector<char> host;
@@ -376,8 +380,13 @@ void nbg_server::run() {
         while (launch_batch(lk)) launched = true;
         if (launched || wake) continue;  // wake: something happened while the lock was dropped
         // woken by a submission or a batch's completion callback; the timeout
-        // is only a backstop
-        cv_work.wait_for(lk, std::chrono::milliseconds(flights.empty() ? 5 : 2));
+        // is a backstop, and the moment the oldest held request's hold ends
+        double wait_us = flights.empty() ? 5000.0 : 2000.0;
+        if (!pending.empty()) {
+            const double left = reqs[pending.front()].t_submit + hold_us() - now_us();
+            wait_us = std::max(50.0, std::min(wait_us, left));
+        }
+        cv_work.wait_for(lk, std::chrono::microseconds((int64_t)wait_us));
     }
 }
 
@@ -414,6 +423,15 @@ static int submit(nbg_server* s, const nbg_desc* d, bool host, int64_t* ticket) 
     if (!d->r || !d->a || d->m < 1) return fail(NBG_EINVAL, "bad request");
     const bool sqr = d->b == nullptr || (d->b == d->a && d->n == d->m);
     if (!sqr && d->n < 1) return fail(NBG_EINVAL, "bad request");
+    {  // the result must not overlap an operand (src/fpntt.jl:979-981)
+        const char* rp = (const char*)d->r;
+        const char* ap = (const char*)d->a;
+        const char* bp = (const char*)d->b;
+        const int64_t n = sqr ? d->m : d->n;
+        const size_t rb = 8 * (size_t)(d->m + n);
+        if ((rp < ap + 8 * (size_t)d->m && ap < rp + rb) || (!sqr && rp < bp + 8 * (size_t)n && bp < rp + rb))
+            return fail(NBG_EINVAL, "r must not alias a or b");
+    }
     q.a = d->a;
     q.b = sqr ? d->a : d->b;
     q.r = d->r;

@@ -40,6 +40,7 @@ EXPORTS = [
     "nbg_server_stats", "nbg_server_destroy",
     "nbg_powermod_batch", "nbg_powermod_batch_dev", "nbg_barrett_mu", "nbg_powmod_schedule",
     "nbg_mullo", "nbg_sqrlo", "nbg_matrix22_mul_dev", "nbg_mul2add_dev", "nbg_radix_combine",
+    "nbg_kernel_arch",
 ]
 
 
@@ -113,6 +114,7 @@ def lib() -> ctypes.CDLL:
             "nbg_mul2add_dev": [vp, i64, vp, i64, vp, i64, vp, i64, vp, i64, vp],
             "nbg_sqrlo": [vp, vp, i64, i64],
             "nbg_powermod_batch_dev": [vp, i64, i64, vp],
+            "nbg_kernel_arch": [c.POINTER(i32)],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -345,7 +347,7 @@ class Batch:
 
 class ServerOpts(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("max_batch", ctypes.c_int64), ("max_queue", ctypes.c_int64),
-                ("batch_points", ctypes.c_int64)]
+                ("batch_points", ctypes.c_int64), ("max_hold_us", ctypes.c_int64)]
 
 
 class ServerStats(ctypes.Structure):
@@ -359,9 +361,9 @@ class Server:
     """Continuous-batching product server (nbg_server_*)."""
 
     def __init__(self, hbm_budget_bytes: int = 1 << 30, max_batch: int = 0, max_queue: int = 0,
-                 batch_points: int = 0):
+                 batch_points: int = 0, max_hold_us: int = 0):
         self._h = ctypes.c_void_p()
-        opts = ServerOpts(hbm_budget_bytes, max_batch, max_queue, batch_points)
+        opts = ServerOpts(hbm_budget_bytes, max_batch, max_queue, batch_points, max_hold_us)
         _check(lib().nbg_server_create(ctypes.byref(opts), ctypes.byref(self._h)))
         self._keep: dict = {}
 

@@ -24,6 +24,7 @@ import time
 
 import numpy as np
 
+from .workload import bits_of, gen_workload
 from . import (Batch, NBGError, get_tuning, lib, make_descs, ntt_params, plan_layout, set_tuning, trim_plans,
                _check, version)
 
@@ -168,8 +169,6 @@ def default_path(name: str) -> str:
 
 
 def main() -> None:
-    import sys
-
     import torch
 
     ap = argparse.ArgumentParser()
@@ -177,17 +176,14 @@ def main() -> None:
     ap.add_argument("--products", type=int, default=10000)
     ap.add_argument("--seed", type=int, default=1)
     args = ap.parse_args()
-    root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-    sys.path.insert(0, root)
-    import bench  # the workload generator of the benchmark
 
     _check(lib().nbg_init(torch.cuda.current_device()))
-    W = bench.gen_workload(args.seed, args.products)
+    W = gen_workload(args.seed, args.products)
     shapes = []
     for k in range(args.products):
         m, n, sq = int(W["m"][k]), int(W["n"][k]), bool(W["sq"][k])
-        ba = bench.bits_of(W["limbs"], int(W["off_a"][k]), m)
-        bb = ba if sq else bench.bits_of(W["limbs"], int(W["off_b"][k]), n)
+        ba = bits_of(W["limbs"], int(W["off_a"][k]), m)
+        bb = ba if sq else bits_of(W["limbs"], int(W["off_b"][k]), n)
         shapes.append((ba, bb, sq))
     # the single-product sizes of the large-product configuration
     for lg in (16, 20, 24):

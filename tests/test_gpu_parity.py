@@ -29,6 +29,16 @@ def bits_equal(x: np.ndarray, y: np.ndarray) -> bool:
     return np.array_equal(np.asarray(x, dtype=np.float64).view(np.uint64), np.asarray(y, dtype=np.float64).view(np.uint64))
 
 
+def test_kernels_are_the_sm100a_build(gpu_lib):
+    # the runtime loaded the kernels' sm_100a machine code (binaryVersion 100),
+    # not a JIT of some other architecture's PTX
+    import ctypes
+
+    v = ctypes.c_int32(0)
+    gpu_lib._check(gpu_lib.lib().nbg_kernel_arch(ctypes.byref(v)))
+    assert v.value == 100
+
+
 @pytest.fixture
 def tuned(gpu_lib):
     """Restores the default pass split after a test that changes it."""

@@ -28,12 +28,6 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) == set(nbgpu.EXPORTS)
 
 
-def test_library_is_sm100a_build():
-    # the fatbin must hold sm_100a code; check the ELF for the arch tag string
-    data = open(nbgpu.LIB_PATH, "rb").read()
-    assert b"sm_100a" in data
-
-
 def test_ntt_len_matches_oracle():
     for T in list(range(1, 5000, 7)) + [15 << 14, (15 << 14) + 1, 7 << 10, 9 << 10, (1 << 34) + 1,
                                        33 << 34, 53 << 34, 315 << 34]:

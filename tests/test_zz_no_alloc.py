@@ -81,3 +81,65 @@ def test_noalloc_rejects_oversized_products(gpu_lib):
     # the array is still usable afterwards
     b = rand_limbs(rng, 500)
     assert np.array_equal(_noalloc(gpu_lib, b, None), _regular(gpu_lib, b, None))
+
+
+_FRESH = r"""
+import sys
+import numpy as np
+import torch
+sys.path.insert(0, {pkg!r})
+import nbgpu
+
+rng = np.random.default_rng(406)
+def rl(n):
+    a = rng.integers(0, 2**64, n, dtype=np.uint64)
+    a[-1] |= np.uint64(1)
+    return a
+# one-pass product, multi-pass products of two lengths, a square: four transform lengths
+shapes = [(rl(700), rl(500)), (rl(3000), rl(2500)), (rl(20000), rl(12000)), (np.full(9000, 2**64 - 1, dtype=np.uint64), None)]
+dev = []
+for a, b in shapes:
+    n = a.size if b is None else b.size
+    dev.append((torch.from_numpy(a).cuda(), None if b is None else torch.from_numpy(b).cuda(),
+                torch.zeros(a.size + n, dtype=torch.uint64, device="cuda"), a.size, n))
+st = torch.cuda.current_stream().cuda_stream
+def call(i):
+    da, db, r, m, n = dev[i]
+    nbgpu.mul_dev_noalloc(r, da, m, db, n, st)
+# warm-up: every kernel these shapes use is loaded and has its local memory
+for i in range(len(dev)):
+    call(i)
+torch.cuda.synchronize()
+want = [dev[i][2].cpu().numpy().copy() for i in range(len(dev))]
+free0, reserved0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()
+for order in ([3, 2, 1, 0], [0, 2, 0, 3, 1], [1, 1, 3, 0, 2]):
+    for i in order:
+        dev[i][2].fill_(7)
+        torch.cuda.synchronize()
+        call(i)
+        torch.cuda.synchronize()
+        assert np.array_equal(dev[i][2].cpu().numpy(), want[i]), i
+free1, reserved1 = torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()
+assert free1 == free0, (free0, free1)
+assert reserved1 == reserved0, (reserved0, reserved1)
+print("noalloc-fresh-ok", free0 - free1)
+"""
+
+
+def test_noalloc_allocates_nothing_in_a_fresh_process():
+    # A process that only ever calls the allocation-free entry point: after one
+    # warm-up call per shape, further calls of four transform lengths in
+    # changing order leave the device's free memory and torch's reserved
+    # memory exactly as they were.
+    import os
+    import subprocess
+    import sys
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from conftest import ROOT
+
+    src = _FRESH.format(pkg=os.path.join(ROOT, "nativebigint.jl_b200"))
+    r = subprocess.run([sys.executable, "-c", src], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "noalloc-fresh-ok" in r.stdout

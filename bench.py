@@ -146,6 +146,30 @@ def cpu_rate(W, idx: list[int], threads: int) -> tuple[float, float]:
     return total / dt, dt
 
 
+def gmp_rate(W, idx: list[int], threads: int) -> tuple[float, float]:
+    """GMP 6.3 mpn_mul / mpn_sqr (the arithmetic of Julia's BigInt) on the
+    same products, `threads` host threads; returns (output limbs/s, seconds)."""
+    import oracle
+
+    limbs = W["limbs"]
+    oracle.gmp()
+
+    def one(k):
+        m, n = int(W["m"][k]), int(W["n"][k])
+        a = limbs[W["off_a"][k]: W["off_a"][k] + m]
+        if W["sq"][k]:
+            oracle.gmp_sqr(a)
+        else:
+            oracle.gmp_mul(a, limbs[W["off_b"][k]: W["off_b"][k] + n])
+        return m + n
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        total = sum(ex.map(one, sorted(idx, key=lambda k: -int(W["m"][k] + W["n"][k]))))
+    dt = time.perf_counter() - t0
+    return total / dt, dt
+
+
 def cpu_sample(W, budget_s: float, threads: int) -> tuple[list[int], str]:
     """A bounded prefix of the workload sized for ~budget_s of CPU work."""
     # single-thread cost model: ~4.5e-7 s per output limb for this size mix (oracle, scalar)
@@ -203,6 +227,26 @@ def fp64_peak() -> dict:
     return {"dfma_per_s": fma.value, "dadd_per_s": add.value}
 
 
+def rank_share(W: dict, rank: int, world: int, scaling: str, params) -> list[int]:
+    """Products of workload W that this rank runs.  weak: every rank draws its
+    own batch (seed + rank), so it runs all of W.  strong: every rank draws the
+    same batch and runs its LPT share by reference-schedule cost
+    (nbgpu/shard.py); the shares are disjoint and cover the batch, and no
+    exchange is needed to agree on them.  `params` is fp_ntt_params."""
+    count = len(W["m"])
+    if scaling == "weak" or world == 1:
+        return list(range(count))
+    from nbgpu import shard
+
+    prods = []
+    for k in range(count):
+        m, n, sq = int(W["m"][k]), int(W["n"][k]), bool(W["sq"][k])
+        ba = bits_of(W["limbs"], int(W["off_a"][k]), m)
+        bb = ba if sq else bits_of(W["limbs"], int(W["off_b"][k]), n)
+        prods.append((ba, bb, sq))
+    return shard.shard(prods, rank, world, params)
+
+
 def hbm_peak() -> tuple[float, str]:
     """HBM copy bandwidth for the byte roofline: MEASURED_PEAKS.json's hbm_gbs
     when that file is present, else the pool's earlier measured fallback."""
@@ -244,15 +288,17 @@ def run_ours(args, rank: int, world: int) -> None:
     nbgpu._check(nbgpu.lib().nbg_init(dev))
     stream = torch.cuda.Stream()
     shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else None
-    W = gen_workload(args.seed + rank, args.products, shape, args.square)
-    count = args.products
+    weak = args.scaling == "weak"
+    W = gen_workload(args.seed + (rank if weak else 0), args.products, shape, args.square)
+    mine = rank_share(W, rank, world, args.scaling, nbgpu.ntt_params)
+    count = len(mine)
     limbs = W["limbs"]
     d_in = torch.from_numpy(limbs).to(f"cuda:{dev}")
     d_out = torch.zeros(W["out_total"], dtype=torch.uint64, device=f"cuda:{dev}")
     ib, ob = d_in.data_ptr(), d_out.data_ptr()
     items = []
     point_primes = 0.0  # sum over products of transform length x 2 primes
-    for k in range(count):
+    for k in mine:
         m, n, sq = int(W["m"][k]), int(W["n"][k]), bool(W["sq"][k])
         ba = bits_of(limbs, int(W["off_a"][k]), m)
         bb = ba if sq else bits_of(limbs, int(W["off_b"][k]), n)
@@ -262,7 +308,7 @@ def run_ours(args, rank: int, world: int) -> None:
     descs = nbgpu.make_descs(items)
     torch.cuda.synchronize()
     bt = nbgpu.Batch(descs)
-    out_limbs = W["out_total"]
+    out_limbs = int(sum(int(W["m"][k] + W["n"][k]) for k in mine))
     s = stream.cuda_stream
 
     # warm-up
@@ -289,18 +335,19 @@ def run_ours(args, rank: int, world: int) -> None:
     step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     total_ms = evs[0].elapsed_time(evs[-1])
     t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
-    units = torch.tensor([float(out_limbs) * args.steps], dtype=torch.float64, device=f"cuda:{dev}")
+    units = torch.tensor([float(out_limbs) * args.steps, float(count)], dtype=torch.float64, device=f"cuda:{dev}")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.all_reduce(units, op=dist.ReduceOp.SUM)
     total_ms_max = float(t.item())
-    value = float(units.item()) / (total_ms_max / 1e3)
+    value = float(units[0].item()) / (total_ms_max / 1e3)
+    job_products = int(units[1].item())
 
     # bit-exactness of this run's results: a seeded sample against GMP
     import oracle
 
     res = d_out.cpu().numpy()
-    chk = np.random.default_rng(5).choice(count, min(args.check, count), replace=False)
+    chk = np.asarray(mine)[np.random.default_rng(5).choice(count, min(args.check, count), replace=False)]
     bad = 0
     for k in chk:
         m, n = int(W["m"][k]), int(W["n"][k])
@@ -357,12 +404,12 @@ def run_ours(args, rank: int, world: int) -> None:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ul = 0
-        for k in range(nb if nb > 0 else 0):
-            one[0] = descs[k]
+        for i in range(nb if nb > 0 else 0):
+            one[0] = descs[i]
             c0 = time.perf_counter()
             nbgpu.mul_batch_dev(one, s)
             lat.append(1e3 * (time.perf_counter() - c0))
-            ul += int(W["m"][k] + W["n"][k])
+            ul += int(W["m"][mine[i]] + W["n"][mine[i]])
         torch.cuda.synchronize()
         un_s = time.perf_counter() - t0
         if nb > 0:
@@ -375,7 +422,7 @@ def run_ours(args, rank: int, world: int) -> None:
         pin_out = torch.zeros(W["out_total"], dtype=torch.uint64).pin_memory()
         hib, hob = pin_in.data_ptr(), pin_out.data_ptr()
         hitems = []
-        for k in range(count):
+        for k in mine:
             m, n, sq = int(W["m"][k]), int(W["n"][k]), bool(W["sq"][k])
             hitems.append((hob + 8 * int(W["out_off"][k]), hib + 8 * int(W["off_a"][k]),
                            None if sq else hib + 8 * int(W["off_b"][k]), m, n, 0, 0))
@@ -391,6 +438,26 @@ def run_ours(args, rank: int, world: int) -> None:
         e2e_val = out_limbs / statistics.median(e2e_t)
         if not np.array_equal(pin_out.numpy(), res):
             raise SystemExit("bench: e2e results differ from the device-resident batch")
+        # the same from pageable host buffers (what a Julia Memory{UInt64} is)
+        pg_out = np.zeros(W["out_total"], dtype=np.uint64)
+        pib, pob = limbs.ctypes.data, pg_out.ctypes.data
+        pitems = []
+        for k in mine:
+            m, n, sq = int(W["m"][k]), int(W["n"][k]), bool(W["sq"][k])
+            pitems.append((pob + 8 * int(W["out_off"][k]), pib + 8 * int(W["off_a"][k]),
+                           None if sq else pib + 8 * int(W["off_b"][k]), m, n, 0, 0))
+        pdescs = nbgpu.make_descs(pitems)
+        nbgpu._check(L.nbg_mul_batch(ctypes.cast(pdescs, ctypes.c_void_p), count))
+        pg_t = []
+        for _ in range(max(2, min(args.steps, 3))):
+            t0 = time.perf_counter()
+            nbgpu._check(L.nbg_mul_batch(ctypes.cast(pdescs, ctypes.c_void_p), count))
+            pg_t.append(time.perf_counter() - t0)
+        if not np.array_equal(pg_out, res):
+            raise SystemExit("bench: pageable e2e results differ from the device-resident batch")
+        e2e_pageable = {"value": out_limbs / statistics.median(pg_t), "unit": "output limbs/s",
+                        "h2d_bytes_per_step": int(8 * len(limbs)), "d2h_bytes_per_step": int(8 * out_limbs),
+                        "buffers": "pageable numpy arrays through nbg_mul_batch"}
 
         # CPU baseline on a bounded sample
         threads = os.cpu_count() or 1
@@ -398,30 +465,42 @@ def run_ours(args, rank: int, world: int) -> None:
         if args.cpu_seconds > 0:
             idx, desc = cpu_sample(W, args.cpu_seconds, threads)
             cpu_v, _ = cpu_rate(W, idx, threads)
+            gmp_v, _ = gmp_rate(W, idx, threads)
             cpu_base = {"value": cpu_v, "unit": "output limbs/s", "cores": threads, "kind": "port",
-                        "sample": desc + "; CPU restatement of src/fpntt.jl (Julia is not installed)"}
+                        "sample": desc + "; CPU restatement of src/fpntt.jl (Julia is not installed)",
+                        "gmp": {"value": gmp_v, "unit": "output limbs/s", "cores": threads,
+                                "sample": "the same products through GMP 6.3 mpn_mul / mpn_sqr"}}
 
+        single_2p24 = None
+        if args.single_2p24:
+            single_2p24 = single_case(24, True, "uniform", max(20, args.steps), peak["dfma_per_s"], stream,
+                                      check="residues")
         clocks = clk.summary()
         med = statistics.median(step_ms)
         line = {
             "metric": METRIC, "value": value, "unit": "output limbs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "products": count, "seed": args.seed,
+            "scaling": args.scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "products": job_products, "products_per_rank": count,
+                       "seed": args.seed,
                        "output_limbs_per_step": out_limbs, "l2": "inputs larger than L2 (0.7 GB operands, 9 GB workspace)",
-                       "parallelism": f"batch shards x{world}, no collective"},
+                       "parallelism": (f"{world} ranks, each its own seeded batch (seed + rank), no collective"
+                                       if args.scaling == "weak" else
+                                       f"one batch split by LPT cost over {world} ranks, no collective")},
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-            "products_per_s": count * world / (total_ms_max / args.steps / 1e3),
+            "products_per_s": job_products / (total_ms_max / args.steps / 1e3),
             "vs_unbatched": value / world / unbatched["value"] if unbatched else None,
             "unbatched": unbatched,
             "bitexact": {"checked_vs_gmp": int(len(chk)), "mismatches": bad},
             "e2e": {"value": e2e_val, "unit": "output limbs/s",
                     "h2d_bytes_per_step": int(8 * len(limbs)), "d2h_bytes_per_step": int(8 * out_limbs)},
+            "e2e_pageable": e2e_pageable,
             "gpu_launches": int(launches),
             "clocks": clocks,
             "roofline": roof,
             "cpu_baseline": cpu_base,
             "median_step_ms": med,
+            "single_2p24_sqr": single_2p24 if args.single_2p24 else None,
         }
         print(json.dumps(line), flush=True)
     bt.close()
@@ -686,19 +765,146 @@ def run_powmod(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_single(args) -> None:
-    """Single large products (balanced mul and sqr at 2^16, 2^20, 2^24 limbs;
-    uniform, all-ones and 1%-sparse limbs), each on the plain one-per-call
+def single_operands(lg: int, kind: str) -> list[np.ndarray]:
+    """Two 2^lg-limb operands: uniform, all-ones or 1%-sparse limbs, top limb nonzero."""
+    n = 1 << lg
+    rng = np.random.Generator(np.random.PCG64(1000 + lg))
+    ops = []
+    for _ in range(2):
+        if kind == "uniform":
+            x = rng.integers(0, 2**64, n, dtype=np.uint64)
+        elif kind == "ones":
+            x = np.full(n, 2**64 - 1, dtype=np.uint64)
+        else:
+            x = np.zeros(n, dtype=np.uint64)
+            idx = rng.choice(n, n // 100, replace=False)
+            x[idx] = rng.integers(1, 2**64, idx.size, dtype=np.uint64)
+        x[-1] |= np.uint64(1)
+        ops.append(x)
+    return ops
+
+
+RESIDUE_MODULI = (2**61 - 1, 2**64 - 59, 2**127 - 1, 10**18 + 9)
+
+
+def residues_agree(a: np.ndarray, b: np.ndarray | None, r: np.ndarray) -> bool:
+    """r == a*b (a^2 when b is None) modulo four fixed moduli: a size-independent
+    check for products too large to recompute in the timed run."""
+    A = int.from_bytes(a.tobytes(), "little")
+    B = A if b is None else int.from_bytes(b.tobytes(), "little")
+    R = int.from_bytes(r.tobytes(), "little")
+    return all((A % q) * (B % q) % q == R % q for q in RESIDUE_MODULI)
+
+
+def single_case(lg: int, sq: bool, kind: str, reps: int, peak: float, s, check: str = "gmp",
+                gmp_time: bool = False) -> dict:
+    """One balanced 2^lg-limb product or square on the plain one-per-call
     device path (nbg_mul_dev / nbg_sqr_dev: plan lookup, job build, launches)
-    and as a captured one-product batch (graph replay).  >= 20 timed
-    repetitions after warm-up, p50/p99 by CUDA events on the calling stream;
-    roofline = the reference schedule's FP64 instructions / p50 time against
-    the FP64 issue rate measured in this run; GMP mpn_mul/mpn_sqr on one host
-    core beside it (uniform pattern).  One JSON line per case."""
+    and as a captured one-product batch (graph replay).  3 warm-up calls, then
+    `reps` timed ones, each by CUDA events on stream `s`; SM clocks sampled
+    during the graph replays.  Roofline: the reference schedule's FP64
+    instructions / p50 time, against `peak` (the DFMA issue rate measured in
+    this run) and against 148 SMs x 64 DFMA per clock x the sampled clock.
+    check: "gmp" compares with mpn_mul / mpn_sqr, "residues" with four
+    residues (see residues_agree)."""
     import torch
 
     import nbgpu
-    import oracle
+
+    n = 1 << lg
+    ops = single_operands(lg, kind)
+    da, db = (torch.from_numpy(x).cuda() for x in ops)
+    r = torch.empty(2 * n, dtype=torch.uint64, device="cuda")
+    ba = 64 * (n - 1) + int(ops[0][-1]).bit_length()
+    bb = ba if sq else 64 * (n - 1) + int(ops[1][-1]).bit_length()
+    descs = nbgpu.make_descs([(r.data_ptr(), da.data_ptr(), None if sq else db.data_ptr(), n, n, ba, bb)])
+    torch.cuda.synchronize()
+
+    def call():
+        if sq:
+            nbgpu.sqr_dev(r, da, n, s)
+        else:
+            nbgpu.mul_dev(r, da, n, db, n, s)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        out = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            e1.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return out
+
+    t_call = timed(call)
+    bt = nbgpu.Batch(descs)
+    dev = torch.cuda.current_device()
+    with ClockSampler(dev) as clk:
+        t_graph = timed(lambda: bt.run(s.cuda_stream))
+    alg = sum(x["alg_ops"] for x in bt.stats())
+    per_kernel = {}
+    prof = [bt.profile(s) for _ in range(3)]
+    for st_, ms in zip(bt.stats(), [statistics.mean(p[i] for p in prof) for i in range(len(prof[0]))]):
+        d = per_kernel.setdefault(st_["kind"], {"ms": 0.0, "alg_ops": 0.0, "launches": 0})
+        d["ms"] += ms
+        d["alg_ops"] += st_["alg_ops"]
+        d["launches"] += 1
+    for d in per_kernel.values():
+        d["frac"] = d["alg_ops"] / (d["ms"] / 1e3) / peak if d["ms"] else 0.0
+    bt.close()
+    got = r.cpu().numpy()
+    if check == "gmp":
+        import oracle
+
+        want = oracle.gmp_sqr(ops[0]) if sq else oracle.gmp_mul(ops[0], ops[1])
+        ok = bool(np.array_equal(got, want))
+    else:
+        ok = residues_agree(ops[0], None if sq else ops[1], got)
+    if not ok:
+        raise SystemExit(f"single: 2^{lg} {kind} {'sqr' if sq else 'mul'} result is wrong ({check})")
+    gmp_ms = None
+    if gmp_time:
+        import oracle
+
+        t0 = time.perf_counter()
+        oracle.gmp_sqr(ops[0]) if sq else oracle.gmp_mul(ops[0], ops[1])
+        gmp_ms = 1e3 * (time.perf_counter() - t0)
+    p50g = float(np.percentile(t_graph, 50))
+    clocks = clk.summary()
+    nominal = 148 * 64 * clocks["sm_mhz"] * 1e6 if clocks.get("sm_mhz") else None
+    del da, db, r
+    torch.cuda.empty_cache()
+    return {
+        "op": "sqr" if sq else "mul", "limbs": n, "pattern": kind,
+        "per_call_p50_ms": float(np.percentile(t_call, 50)), "per_call_p99_ms": float(np.percentile(t_call, 99)),
+        "graph_p50_ms": p50g, "graph_p99_ms": float(np.percentile(t_graph, 99)),
+        "output_limbs_per_s": 2 * n / (p50g / 1e3),
+        "roofline": {"bound": "fp64", "alg_ops": alg, "achieved": alg / (p50g / 1e3) / 1e12,
+                     "peak": peak / 1e12, "unit": "T FP64 instr/s", "frac": alg / (p50g / 1e3) / peak,
+                     "peak_source": "measured: DFMA issue rate of libnbgpu_peak.so in this run",
+                     "frac_of_nominal": alg / (p50g / 1e3) / nominal if nominal else None,
+                     "nominal_source": "148 SMs x 64 DFMA/clock x median sampled SM clock",
+                     "kernels": per_kernel},
+        "check": {"kind": check, "ok": ok},
+        "clocks": clocks,
+        "cpu_baseline": None if gmp_ms is None else {"value": gmp_ms, "unit": "ms", "cores": 1,
+                                                      "kind": "gmp", "sample": "one call, GMP 6.3 mpn"},
+        "reps": reps,
+    }
+
+
+def run_single(args) -> None:
+    """Single large products (balanced mul and sqr at --single-sizes, 2^16,
+    2^20, 2^24 limbs by default; uniform, all-ones and 1%-sparse limbs), see
+    single_case; GMP mpn_mul/mpn_sqr on one host core beside the uniform
+    pattern.  One JSON line per case."""
+    import torch
+
+    import nbgpu
 
     torch.cuda.set_device(0)
     nbgpu._check(nbgpu.lib().nbg_init(0))
@@ -706,82 +912,19 @@ def run_single(args) -> None:
     s = torch.cuda.Stream()
     reps = max(20, args.steps)
     lgs = [int(x) for x in args.single_sizes.split(",")]
+    kinds = args.single_patterns.split(",")
+    opsel = args.single_ops.split(",")
     for lg in lgs:
-        n = 1 << lg
-        for kind in ("uniform", "ones", "sparse"):
-            rng = np.random.Generator(np.random.PCG64(1000 + lg))
-            ops = []
-            for _ in range(2):
-                if kind == "uniform":
-                    x = rng.integers(0, 2**64, n, dtype=np.uint64)
-                elif kind == "ones":
-                    x = np.full(n, 2**64 - 1, dtype=np.uint64)
-                else:
-                    x = np.zeros(n, dtype=np.uint64)
-                    idx = rng.choice(n, n // 100, replace=False)
-                    x[idx] = rng.integers(1, 2**64, idx.size, dtype=np.uint64)
-                x[-1] |= np.uint64(1)
-                ops.append(x)
-            da, db = (torch.from_numpy(x).cuda() for x in ops)
+        for kind in kinds:
             for sq in (False, True):
-                r = torch.empty(2 * n, dtype=torch.uint64, device="cuda")
-                ba = 64 * (n - 1) + int(ops[0][-1]).bit_length()
-                bb = ba if sq else 64 * (n - 1) + int(ops[1][-1]).bit_length()
-                descs = nbgpu.make_descs([(r.data_ptr(), da.data_ptr(), None if sq else db.data_ptr(), n, n, ba, bb)])
-                torch.cuda.synchronize()
-
-                def call():
-                    if sq:
-                        nbgpu.sqr_dev(r, da, n, s)
-                    else:
-                        nbgpu.mul_dev(r, da, n, db, n, s)
-
-                def timed(fn):
-                    for _ in range(3):
-                        fn()
-                    torch.cuda.synchronize()
-                    out = []
-                    for _ in range(reps):
-                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                        e0.record(s)
-                        fn()
-                        e1.record(s)
-                        e1.synchronize()
-                        out.append(e0.elapsed_time(e1))
-                    return out
-
-                t_call = timed(call)
-                bt = nbgpu.Batch(descs)
-                t_graph = timed(lambda: bt.run(s.cuda_stream))
-                alg = sum(x["alg_ops"] for x in bt.stats())
-                bt.close()
-                got = r.cpu().numpy()
-                a0 = ops[0]
-                want = oracle.gmp_sqr(a0) if sq else oracle.gmp_mul(a0, ops[1])
-                if not np.array_equal(got, want):
-                    raise SystemExit(f"single: 2^{lg} {kind} {'sqr' if sq else 'mul'} differs from GMP")
-                gmp_ms = None
-                if kind == "uniform":
-                    t0 = time.perf_counter()
-                    oracle.gmp_sqr(a0) if sq else oracle.gmp_mul(a0, ops[1])
-                    gmp_ms = 1e3 * (time.perf_counter() - t0)
-                p50g = float(np.percentile(t_graph, 50))
-                line = {
-                    "mode": "single", "impl": "ours", "op": "sqr" if sq else "mul", "limbs": n, "pattern": kind,
-                    "metric": "single large product time, bit-exact vs GMP", "unit": "ms", "higher_is_better": False,
-                    "per_call_p50_ms": float(np.percentile(t_call, 50)), "per_call_p99_ms": float(np.percentile(t_call, 99)),
-                    "graph_p50_ms": p50g, "graph_p99_ms": float(np.percentile(t_graph, 99)),
-                    "output_limbs_per_s": 2 * n / (p50g / 1e3),
-                    "roofline": {"bound": "fp64", "alg_ops": alg, "achieved": alg / (p50g / 1e3) / 1e12,
-                                 "peak": peak / 1e12, "unit": "T FP64 instr/s", "frac": alg / (p50g / 1e3) / peak,
-                                 "peak_source": "measured: DFMA issue rate of libnbgpu_peak.so in this run"},
-                    "cpu_baseline": None if gmp_ms is None else {"value": gmp_ms, "unit": "ms", "cores": 1,
-                                                                  "kind": "gmp", "sample": "one call, GMP 6.3 mpn"},
-                    "reps": reps, "dtype": "f64", "data": "synthetic", "n_gpus": 1,
-                }
+                if ("sqr" if sq else "mul") not in opsel:
+                    continue
+                rec = single_case(lg, sq, kind, reps, peak, s, check=args.single_check,
+                                  gmp_time=kind == "uniform" and args.single_check == "gmp")
+                line = {"mode": "single", "impl": "ours",
+                        "metric": "single large product time, bit-exact", "unit": "ms", "higher_is_better": False,
+                        **rec, "dtype": "f64", "data": "synthetic", "n_gpus": 1}
                 print(json.dumps(line), flush=True)
-            del da, db
-            torch.cuda.empty_cache()
 
 
 def run_route(args) -> None:
@@ -839,6 +982,9 @@ def main() -> None:
     ap.add_argument("--route", action="store_true", help="per-call timings of products below NTT admission")
     ap.add_argument("--single", action="store_true", help="single large products at --single-sizes")
     ap.add_argument("--single-sizes", default="16,20,24", help="log2 limb counts")
+    ap.add_argument("--single-patterns", default="uniform,ones,sparse")
+    ap.add_argument("--single-ops", default="mul,sqr")
+    ap.add_argument("--single-check", default="gmp", choices=["gmp", "residues"])
     ap.add_argument("--powmod-chains", type=int, default=256)
     ap.add_argument("--powmod-ebits", type=int, default=4096, help="exponent bits (a multiple of 64)")
     ap.add_argument("--serve", action="store_true", help="serving loop at swept Poisson arrival rates")
@@ -846,9 +992,26 @@ def main() -> None:
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-pool", type=int, default=600)
     ap.add_argument("--serve-budget-gb", type=float, default=60.0)
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="weak: each rank runs its own batch; strong: ranks split one batch by cost")
+    ap.add_argument("--single-2p24", type=int, default=1,
+                    help="1: the default line also times one 2^24-limb square (its FP64 roofline)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.gpus > 1 and world == 1 and "RANK" not in os.environ:
+        # one process per GPU: relaunch this command under torchrun
+        import socket
+
+        sk = socket.socket()
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+        sk.close()
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+        raise SystemExit(subprocess.call(cmd))
+    if world > 1 and args.gpus != world:
+        raise SystemExit(f"bench: --gpus {args.gpus} but WORLD_SIZE {world}")
     if world > 1:
         import datetime
 

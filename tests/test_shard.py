@@ -83,3 +83,41 @@ def test_cost_model_matches_counted_ops():
         bch, N = O.ntt_params(ba, bb)
         nconv = -(-ba // bch) + -(-bb // bch) - 1
         assert shard.product_cost(N, sq, nconv) == O.op_count_product(a, b)
+
+
+def _bench_worker(rank, world, port, q):
+    # the benchmark's own rank logic (bench.rank_share) under gloo ranks
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import bench
+        import nbgpu
+
+        W = bench.gen_workload(1, 600)
+        strong = bench.rank_share(W, rank, world, "strong", nbgpu.ntt_params)
+        weak = bench.rank_share(W, rank, world, "weak", nbgpu.ntt_params)
+        got = [None] * world
+        dist.all_gather_object(got, (strong, len(weak)))
+        if rank == 0:
+            q.put(got)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_rank_logic_two_gloo_ranks():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bench_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=180)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    parts = [g[0] for g in got]
+    assert sorted(i for part in parts for i in part) == list(range(600))  # strong: disjoint cover of one batch
+    assert all(g[1] == 600 for g in got)                                # weak: each rank its whole own batch
+    assert min(len(p) for p in parts) > 100

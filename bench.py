@@ -518,15 +518,18 @@ def run_serve(args) -> None:
     the pool, so each generation writes every pool slot once; the results go to
     one of RING copies of the pool's output area, and before a copy is reused
     every request that wrote it is waited for and the whole copy is compared
-    with the GMP products on the device (every result is checked).  Latency is
-    the server's submit-to-completion time; `submit_lag` is how far the Python
-    submission loop fell behind the Poisson schedule."""
+    with the GMP products on the device (every result is checked).  Requests
+    are submitted by libnbgpu_loadgen.so at their Poisson arrival times, one
+    generation per call; between generations the benchmark waits for and checks
+    the generation that last used the next ring copy (a stall when the server
+    is behind).  Latency is the server's submit-to-completion time;
+    `submit_lag` is how far submission fell behind the arrival schedule."""
     import torch
 
     import nbgpu
     import oracle
 
-    RING = 4
+    RING = args.serve_ring
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     L = nbgpu.lib()
@@ -589,69 +592,72 @@ def run_serve(args) -> None:
         idx = torch.as_tensor(np.asarray(slots, dtype=np.int64), device="cuda")
         return int((per[idx] != 0).sum().item())
 
+    lg = ctypes.CDLL(os.path.join(ROOT, "nativebigint.jl_b200", "lib", "libnbgpu_loadgen.so"))
+    lg.nbg_loadgen_now.restype = ctypes.c_double
+    lg.nbg_loadgen_submit.restype = ctypes.c_int
+    lg.nbg_loadgen_submit.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_int64, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.POINTER(ctypes.c_int64)]
     rates = [float(x) for x in args.serve_rates.split(",") if x]
     for rate in rates:
-        srv = nbgpu.Server(hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)))
+        srv = nbgpu.Server(hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_hold_us=args.serve_hold_us)
         h = srv._h
-        ticket = ctypes.c_int64()
         arrivals = np.cumsum(rng.exponential(1.0 / rate, int(rate * args.serve_seconds * 1.05) + 16))
-        arrivals = arrivals[arrivals < args.serve_seconds]
-        gen_tickets: list[list[int]] = []
-        gen_slots: list[list[int]] = []
+        arrivals = arrivals[arrivals < args.serve_seconds][: args.serve_max_requests]
+        count = len(arrivals)
+        ngen = (count + P - 1) // P
+        tickets = np.zeros(count, dtype=np.int64)
+        lags = np.zeros(count, dtype=np.float64)
+        slots = np.zeros(count, dtype=np.int32)
         mismatches, stalls, stall_s = 0, 0, 0.0
-        lags = np.zeros(len(arrivals))
         submitted_limbs = 0
-        perm = None
         for c in range(RING):
             ring[c].zero_()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for i, ta in enumerate(arrivals):
-            g, j = divmod(i, P)
-            if j == 0:
-                perm = rng.permutation(P)
-                if g >= RING:  # reuse ring copy g % RING: its generation must be done, then checked
-                    ts = time.perf_counter()
-                    waited = False
-                    for t in gen_tickets[g - RING]:
-                        if not waited:
-                            done = ctypes.c_int32()
-                            L.nbg_poll(h, t, ctypes.byref(done))
-                            waited = not done.value
-                        nbgpu._check(L.nbg_wait(h, t, 600_000_000))
-                        L.nbg_release(h, t)
-                    stalls += int(waited)
-                    stall_s += time.perf_counter() - ts
-                    mismatches += check_copy(g % RING, gen_slots[g - RING])
-                    ring[g % RING].zero_()
-                    torch.cuda.current_stream().synchronize()
-                gen_tickets.append([])
-                gen_slots.append([])
-            k = int(perm[j])
-            gen_slots[g].append(k)
-            while time.perf_counter() - t0 < ta:
-                pass
-            lags[i] = time.perf_counter() - t0 - ta
-            nbgpu._check(L.nbg_submit_dev(h, ctypes.byref(descs[g % RING], k * ctypes.sizeof(nbgpu.NbgDesc)),
-                                          ctypes.byref(ticket)))
-            gen_tickets[g].append(ticket.value)
-            submitted_limbs += int(m[k] + n[k])
-        t_sub = time.perf_counter() - t0
-        for g in range(max(0, len(gen_tickets) - RING), len(gen_tickets)):
-            for t in gen_tickets[g]:
-                nbgpu._check(L.nbg_wait(h, t, 600_000_000))
-            mismatches += check_copy(g % RING, gen_slots[g])
-        t_all = time.perf_counter() - t0
+        done = ctypes.c_int64()
+        t_start = lg.nbg_loadgen_now() + 0.002
+
+        def retire_gen(g: int) -> int:
+            """Waits for generation g, checks its ring copy against GMP, clears it."""
+            lo, hi = g * P, min((g + 1) * P, count)
+            for t in tickets[lo:hi]:
+                nbgpu._check(L.nbg_wait(h, int(t), 600_000_000))
+                L.nbg_release(h, int(t))
+            bad = check_copy(g % RING, slots[lo:hi])
+            ring[g % RING].zero_()
+            torch.cuda.current_stream().synchronize()
+            return bad
+
+        for g in range(ngen):
+            lo, hi = g * P, min((g + 1) * P, count)
+            if g >= RING:  # ring copy g % RING is reused: its previous generation must be done and checked
+                ts = time.perf_counter()
+                first = ctypes.c_int32()
+                L.nbg_poll(h, int(tickets[(g - RING + 1) * P - 1]), ctypes.byref(first))
+                stalls += int(not first.value)
+                mismatches += retire_gen(g - RING)
+                stall_s += time.perf_counter() - ts
+            slots[lo:hi] = rng.permutation(P)[: hi - lo]
+            rc = lg.nbg_loadgen_submit(h, ctypes.cast(descs[g % RING], ctypes.c_void_p),
+                                       slots[lo:].ctypes.data, arrivals[lo:].ctypes.data, hi - lo, t_start,
+                                       tickets[lo:].ctypes.data, lags[lo:].ctypes.data, ctypes.byref(done))
+            nbgpu._check(rc)
+            submitted_limbs += int((m[slots[lo:hi]] + n[slots[lo:hi]]).sum())
+        t_sub = lg.nbg_loadgen_now() - t_start
+        for g in range(max(0, ngen - RING), ngen):
+            mismatches += retire_gen(g)
+        t_all = lg.nbg_loadgen_now() - t_start
         st = srv.stats()
         srv.close()
-        count = len(arrivals)
         line = {
             "metric": "serving: sustained output limbs/s and submit-to-completion latency", "impl": "ours",
             "mode": "serve", "unit": "output limbs/s", "value": st["output_limbs_per_s"],
             "offered_rate": rate, "submitted_rate": count / t_sub if t_sub > 0 else None,
-            "requests": count, "completed": st["completed"], "failed": st["failed"],
+            "requests": count, "window_s": float(arrivals[-1]) if count else 0.0,
+            "completed": st["completed"], "failed": st["failed"],
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "submit_lag_p99_ms": float(np.percentile(lags, 99) * 1e3) if count else None,
+            "submit_lag_p50_ms": float(np.percentile(lags, 50) / 1e3) if count else None,
+            "submit_lag_p99_ms": float(np.percentile(lags, 99) / 1e3) if count else None,
             "wall_s": t_all, "output_limbs": submitted_limbs,
             "ring_stalls": stalls, "ring_stall_s": stall_s,
             "batches": st["batches"], "mean_batch_requests": st["mean_batch_requests"],
@@ -659,7 +665,9 @@ def run_serve(args) -> None:
             "bitexact": {"checked_vs_gmp": count, "mismatches": mismatches},
             "dtype": "f64", "data": "synthetic", "n_gpus": 1,
             "config": {"workload": SERVE_WORKLOAD, "pool_products": P, "pool_output_limbs": out_total,
-                       "hbm_budget_gb": args.serve_budget_gb, "seconds": args.serve_seconds, "seed": args.seed},
+                       "hbm_budget_gb": args.serve_budget_gb, "seconds": args.serve_seconds, "seed": args.seed,
+                       "max_hold_us": args.serve_hold_us, "ring_copies": RING,
+                       "submitter": "libnbgpu_loadgen.so (native open-loop submission at the arrival times)"},
         }
         print(json.dumps(line), flush=True)
         if mismatches or st["failed"]:
@@ -992,6 +1000,9 @@ def main() -> None:
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-pool", type=int, default=600)
     ap.add_argument("--serve-budget-gb", type=float, default=60.0)
+    ap.add_argument("--serve-hold-us", type=int, default=0, help="server max_hold_us (0: library default)")
+    ap.add_argument("--serve-max-requests", type=int, default=40000, help="cap on requests per rate")
+    ap.add_argument("--serve-ring", type=int, default=8, help="copies of the pool's result area")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="weak: each rank runs its own batch; strong: ranks split one batch by cost")
     ap.add_argument("--single-2p24", type=int, default=1,

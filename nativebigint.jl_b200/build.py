@@ -68,6 +68,11 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     out = os.path.join(LIB, "libnbgpu.so")
     if _stale(out, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", out] + objs + ["-cudart", "static", "-lpthread", "-ldl", "-lrt"])
+    # open-loop request generator of the serving benchmark (links libnbgpu.so)
+    ls = os.path.join(CSRC, "loadgen.cpp")
+    lo = os.path.join(LIB, "libnbgpu_loadgen.so")
+    if _stale(lo, [ls, out]):
+        _run([cxx] + CXX_FLAGS + ["-shared", ls, "-o", lo, f"-L{LIB}", "-lnbgpu", "-Wl,-rpath,$ORIGIN"])
     # FP64 issue-rate probe used by bench.py for the roofline denominator
     ps = os.path.join(CSRC, "peak.cu")
     po = os.path.join(LIB, "libnbgpu_peak.so")

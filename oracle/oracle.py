@@ -256,6 +256,36 @@ def gmp_mul(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     return r
 
 
+class _Mpz(ctypes.Structure):
+    _fields_ = [("alloc", ctypes.c_int), ("size", ctypes.c_int), ("d", ctypes.c_void_p)]
+
+
+def _mpz_from(g, z: _Mpz, a: np.ndarray) -> None:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    g.__gmpz_import(ctypes.byref(z), ctypes.c_size_t(a.size), -1, 8, 0, 0, a.ctypes.data_as(ctypes.c_void_p))
+
+
+def gmp_powm(b: np.ndarray, e: np.ndarray, m: np.ndarray) -> np.ndarray:
+    """b^e mod m through GMP's mpz_powm; the result as m.size limbs.  ctypes
+    releases the GIL, so independent calls run in parallel threads."""
+    g = gmp()
+    zs = [_Mpz() for _ in range(4)]
+    for z in zs:
+        g.__gmpz_init(ctypes.byref(z))
+    try:
+        _mpz_from(g, zs[0], b)
+        _mpz_from(g, zs[1], e)
+        _mpz_from(g, zs[2], m)
+        g.__gmpz_powm(ctypes.byref(zs[3]), ctypes.byref(zs[0]), ctypes.byref(zs[1]), ctypes.byref(zs[2]))
+        out = np.zeros(max(int(np.asarray(m).size), 1) + 1, dtype=np.uint64)
+        cnt = ctypes.c_size_t(0)
+        g.__gmpz_export(out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(cnt), -1, 8, 0, 0, ctypes.byref(zs[3]))
+        return out[: np.asarray(m).size].copy()
+    finally:
+        for z in zs:
+            g.__gmpz_clear(ctypes.byref(z))
+
+
 def gmp_sqr(a: np.ndarray) -> np.ndarray:
     a = np.ascontiguousarray(a, dtype=np.uint64)
     r = np.zeros(2 * len(a), dtype=np.uint64)

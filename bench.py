@@ -972,6 +972,72 @@ def run_route(args) -> None:
     print(json.dumps({"mode": "route", "metric": "per-call us, unbalanced products below NTT admission",
                       "rows": rows, "data": "synthetic", "n_gpus": 1}), flush=True)
 
+    # The per-call crossover above the reference's NTT admission: one
+    # host-buffer call (pageable numpy buffers, as a Julia Memory is) against
+    # GMP on one core, the oracle port on one core, and an estimate of the
+    # reference's own CPU engine (GMP's time x the reference's published
+    # mul!/mpn_mul ratio at that size).
+    import oracle as O
+
+    xrows = []
+    for shape in ("balanced", "quarter", "square"):
+        for m in (152, 304, 608, 1216, 2432, 4864, 9728, 19456, 65536, 262144, 1048576):
+            n = m if shape != "quarter" else max(64, m // 4)
+            a = rng.integers(0, 2**64, m, dtype=np.uint64)
+            b = rng.integers(0, 2**64, n, dtype=np.uint64)
+            a[-1] |= np.uint64(1)
+            b[-1] |= np.uint64(1)
+            sq = shape == "square"
+            gpu = (lambda: nbgpu.sqr(a)) if sq else (lambda: nbgpu.mul(a, b))
+            gmpf = (lambda: O.gmp_sqr(a)) if sq else (lambda: O.gmp_mul(a, b))
+            port = (lambda: O.sqr(a)) if sq else (lambda: O.mul(a, b))
+            if not np.array_equal(gpu(), gmpf()):
+                raise SystemExit(f"route bench: {m}x{n} {shape} differs from GMP")
+            reps = max(3, min(200, int(3e7 / (m * max(1.0, math.log2(m)) * 20))))
+
+            def med(fn, r):
+                ts = []
+                for _ in range(r):
+                    t0 = time.perf_counter()
+                    fn()
+                    ts.append(time.perf_counter() - t0)
+                return 1e6 * statistics.median(ts)
+
+            g_us, m_us = med(gpu, reps), med(gmpf, reps)
+            p_us = med(port, max(1, min(reps, 5)))
+            ref_us = m_us * reference_gmp_ratio(64 * (m + n) // 2)
+            xrows.append({"shape": shape, "m": m, "n": n, "gpu_us": g_us, "gmp_us": m_us, "port_us": p_us,
+                          "reference_estimate_us": ref_us})
+    cross = {}
+    for shape in ("balanced", "quarter", "square"):
+        rs = [r for r in xrows if r["shape"] == shape]
+        cross[shape] = next((r["m"] for i, r in enumerate(rs)
+                             if all(x["gpu_us"] < x["reference_estimate_us"] for x in rs[i:])), None)
+    print(json.dumps({"mode": "route_crossover",
+                      "metric": "per-call us from pageable host buffers: GPU nbg_mul/nbg_sqr vs CPU",
+                      "rows": xrows, "crossover_m": cross,
+                      "reference_estimate": "GMP mpn time x the reference's published mul!/mpn_mul ratio "
+                                            "(README.md:142-148, log-interpolated by operand bits)",
+                      "data": "synthetic", "n_gpus": 1}), flush=True)
+
+
+# The reference's published mul!/__gmpn_mul time ratios for balanced operands
+# by operand bits (NativeBigInt.jl README.md:142-148).
+REFERENCE_GMP_RATIOS = ((10e3, 0.90), (16e3, 0.68), (33e3, 0.52), (49e3, 0.46), (66e3, 0.38), (98e3, 0.35),
+                        (131e3, 0.30), (262e3, 0.29), (524e3, 0.25), (2.1e6, 0.27), (16.8e6, 0.25), (268e6, 0.46))
+
+
+def reference_gmp_ratio(bits: float) -> float:
+    """Log-linear interpolation of REFERENCE_GMP_RATIOS (clamped at the ends)."""
+    pts = REFERENCE_GMP_RATIOS
+    if bits <= pts[0][0]:
+        return pts[0][1]
+    for (b0, r0), (b1, r1) in zip(pts, pts[1:]):
+        if bits <= b1:
+            f = (math.log(bits) - math.log(b0)) / (math.log(b1) - math.log(b0))
+            return r0 + f * (r1 - r0)
+    return pts[-1][1]
+
 
 def main() -> None:
     ap = argparse.ArgumentParser()

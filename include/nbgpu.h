@@ -232,6 +232,15 @@ int nbg_mul2add_dev(uint64_t *r, int64_t rn, const uint64_t *a, int64_t la, cons
  * Host buffers. */
 int nbg_radix_combine(uint64_t *out, int64_t cap, const uint64_t *chunks, int64_t n, uint64_t bb, int64_t *out_len);
 
+/* The power table of radix_chunks_dc (src/nbig.jl:394-399): entry 1 is bb,
+ * entry i+1 the square of entry i, continued while the last entry is <= x
+ * (x[0..xn), host buffer).  Entry i (0-based) is out[offsets[i] ..
+ * offsets[i+1]), normalized; *entries gets the count (offsets needs
+ * max_entries + 1 slots, out `cap` limbs; about 4*xn suffice).  Every square
+ * runs on the GPU, the chain staying on the device. */
+int nbg_radix_powtab(uint64_t *out, int64_t cap, int64_t *offsets, int32_t max_entries, uint64_t bb,
+                     const uint64_t *x, int64_t xn, int32_t *entries);
+
 /* ---- admission (host-side restatement of the reference's sizing) -------- */
 
 /* fp_ntt_params (src/fpntt.jl:964-977): chunk width b and transform length N. */

@@ -457,3 +457,70 @@ extern "C" int nbg_radix_combine(uint64_t* out, int64_t cap, const uint64_t* chu
     *out_len = l;
     return NBG_OK;
 }
+
+// The power table of radix_chunks_dc (src/nbig.jl:394-399): powtab[1] = bb,
+// powtab[i+1] = powtab[i]^2, extended while its last entry is <= x.  Every
+// square runs on the GPU with the chain kept on the device; each new entry's
+// top limb comes back to trim it to its normalized length and to decide
+// whether the table goes on.
+extern "C" int nbg_radix_powtab(uint64_t* out, int64_t cap, int64_t* offsets, int32_t max_entries, uint64_t bb,
+                                const uint64_t* x, int64_t xn, int32_t* entries) {
+    if (!out || !offsets || !entries || !x || xn < 1 || bb < 2 || max_entries < 1 || cap < 1)
+        return fail(NBG_EINVAL, "bad argument");
+    while (xn > 1 && x[xn - 1] == 0) xn--;
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    int rc = g_eng.ensure();
+    if (rc) return rc;
+    cudaStream_t st = g_eng.stream;
+    std::vector<void*> keep;
+    struct Free {
+        std::vector<void*>& k;
+        ~Free() {
+            for (void* p : k) cudaFree(p);
+        }
+    } guard{keep};
+    // is the n-limb value p (host copy) <= x?
+    auto le_x = [&](const uint64_t* p, int64_t n) {
+        if (n != xn) return n < xn;
+        for (int64_t i = n - 1; i >= 0; i--)
+            if (p[i] != x[i]) return p[i] < x[i];
+        return true;
+    };
+    int32_t ne = 0;
+    int64_t used = 0;
+    // entry 1: bb itself
+    out[0] = bb;
+    offsets[0] = 0;
+    used = 1;
+    ne = 1;
+    uint64_t* dprev = nullptr;
+    int64_t plen = 1;
+    LA_TRY(cudaMalloc((void**)&dprev, 8));
+    keep.push_back(dprev);
+    LA_TRY(cudaMemcpyAsync(dprev, &bb, 8, cudaMemcpyHostToDevice, st));
+    bool more = le_x(out, 1);
+    while (more) {
+        if (ne >= max_entries) return fail(NBG_EINVAL, "power table needs more than %d entries", (int)max_entries);
+        uint64_t* dnext = nullptr;
+        LA_TRY(cudaMalloc((void**)&dnext, 8 * (size_t)(2 * plen)));
+        keep.push_back(dnext);
+        if ((rc = nbg_sqr_dev(dnext, dprev, plen, st))) return rc;
+        int64_t nl = 2 * plen;
+        uint64_t top = 0;
+        LA_TRY(cudaMemcpyAsync(&top, dnext + nl - 1, 8, cudaMemcpyDeviceToHost, st));
+        LA_TRY(cudaStreamSynchronize(st));
+        if (top == 0) nl--;  // a square of a normalized value has 2n or 2n-1 limbs
+        if (used + nl > cap) return fail(NBG_EINVAL, "output needs more than %lld limbs", (long long)cap);
+        LA_TRY(cudaMemcpyAsync(out + used, dnext, 8 * (size_t)nl, cudaMemcpyDeviceToHost, st));
+        LA_TRY(cudaStreamSynchronize(st));
+        offsets[ne] = used;
+        more = le_x(out + used, nl);
+        used += nl;
+        ne++;
+        dprev = dnext;
+        plen = nl;
+    }
+    offsets[ne] = used;
+    *entries = ne;
+    return NBG_OK;
+}

@@ -143,6 +143,23 @@ function gpu_radix_combine(chunks::Vector{Limb}, bb::Limb)
     return out, Int(len[])
 end
 
+# radix_chunks_dc's power table (src/nbig.jl:394-399): [bb, bb^2, bb^4, ...]
+# while the last entry is <= x, each square on the GPU (x as limbs, normalized).
+function gpu_radix_powtab(bb::Limb, x::Vector{Limb})
+    cap = 4 * length(x) + 64
+    out = Memory{Limb}(undef, cap)
+    maxe = 70
+    offs = Vector{Int64}(undef, maxe + 1)
+    ne = Ref{Int32}(0)
+    GC.@preserve out offs x begin
+        rc = ccall((:nbg_radix_powtab, LIB), Cint,
+                   (Ptr{Limb}, Int64, Ptr{Int64}, Int32, UInt64, Ptr{Limb}, Int64, Ref{Int32}),
+                   pointer(out), cap, pointer(offs), maxe, bb, pointer(x), length(x), ne)
+    end
+    check(rc)
+    return [out[offs[i]+1:offs[i+1]] for i in 1:Int(ne[])]
+end
+
 # Replaces the engine entry points of the enclosing NativeBigInt module so every
 # NTT-sized mul!/sqr!/mul_bal! (src/mul.jl:134, :146, :161, :388-390) and NBig *
 # (src/nbig.jl:124-140) run on the GPU.

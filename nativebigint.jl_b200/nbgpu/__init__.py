@@ -40,7 +40,7 @@ EXPORTS = [
     "nbg_server_stats", "nbg_server_destroy",
     "nbg_powermod_batch", "nbg_powermod_batch_dev", "nbg_barrett_mu", "nbg_powmod_schedule",
     "nbg_mullo", "nbg_sqrlo", "nbg_matrix22_mul_dev", "nbg_mul2add_dev", "nbg_radix_combine",
-    "nbg_kernel_arch",
+    "nbg_kernel_arch", "nbg_radix_powtab",
 ]
 
 
@@ -115,6 +115,7 @@ def lib() -> ctypes.CDLL:
             "nbg_sqrlo": [vp, vp, i64, i64],
             "nbg_powermod_batch_dev": [vp, i64, i64, vp],
             "nbg_kernel_arch": [c.POINTER(i32)],
+            "nbg_radix_powtab": [vp, i64, c.POINTER(i64), i32, c.c_uint64, vp, i64, c.POINTER(i32)],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -244,6 +245,19 @@ def radix_combine(chunks, bb: int) -> np.ndarray:
     n = ctypes.c_int64()
     _check(lib().nbg_radix_combine(_ptr(out), out.size, _ptr(c), c.size, bb, ctypes.byref(n)))
     return out[: n.value]
+
+
+def radix_powtab(bb: int, x) -> list[np.ndarray]:
+    """radix_chunks_dc's power table for x: [bb, bb^2, bb^4, ...] while the
+    last entry is <= x (normalized limb arrays; squares on the GPU)."""
+    x = _u64(x)
+    cap = 4 * x.size + 64
+    out = np.zeros(cap, dtype=np.uint64)
+    maxe = 70
+    offs = (ctypes.c_int64 * (maxe + 1))()
+    ne = ctypes.c_int32()
+    _check(lib().nbg_radix_powtab(_ptr(out), cap, offs, maxe, int(bb), _ptr(x), x.size, ctypes.byref(ne)))
+    return [out[offs[i]: offs[i + 1]].copy() for i in range(ne.value)]
 
 
 def mul_batch(pairs) -> list[np.ndarray]:

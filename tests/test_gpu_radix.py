@@ -36,3 +36,21 @@ def test_radix_combine_zeros_and_rejects(gpu_lib):
     assert O.to_int(gpu_lib.radix_combine(c, 10**19)) == 7 * 10 ** (19 * 69)
     with pytest.raises(gpu_lib.NBGError):
         gpu_lib.radix_combine(np.array([10], dtype=np.uint64), 10)
+
+
+@pytest.mark.parametrize("bb", [10**19, 2**64 - 1, 3])
+def test_radix_powtab_matches_reference_table(gpu_lib, bb):
+    # radix_chunks_dc's table (src/nbig.jl:396-399): bb^(2^(i-1)) while the last entry <= x
+    rng = np.random.default_rng(710 + bb % 991)
+    for xn in (1, 2, 9, 300, 5000, 70000):
+        x = rng.integers(0, 2**64, xn, dtype=np.uint64)
+        x[-1] |= np.uint64(1)
+        xv = O.to_int(x)
+        want = [bb]
+        while want[-1] <= xv:
+            want.append(want[-1] * want[-1])
+        got = gpu_lib.radix_powtab(bb, x)
+        assert [O.to_int(g) for g in got] == want, (bb, xn)
+        assert all(g.size == 0 or g[-1] != 0 for g in got)  # normalized
+    # x below bb: the table is bb alone
+    assert [O.to_int(g) for g in gpu_lib.radix_powtab(bb, np.array([1], dtype=np.uint64))] == [bb]

@@ -160,15 +160,46 @@ function gpu_radix_powtab(bb::Limb, x::Vector{Limb})
     return [out[offs[i]+1:offs[i+1]] for i in 1:Int(ne[])]
 end
 
-# Replaces the engine entry points of the enclosing NativeBigInt module so every
-# NTT-sized mul!/sqr!/mul_bal! (src/mul.jl:134, :146, :161, :388-390) and NBig *
-# (src/nbig.jl:124-140) run on the GPU.
-function install!(mod::Module = parentmodule(@__MODULE__))
+# Per-call crossover of the drop-in hook: one host-buffer call (pageable
+# Memory, copies included) against the reference's CPU engine.  A product goes
+# to the GPU when its smaller operand has at least GPU_MIN_LIMBS limbs (squares:
+# GPU_MIN_SQR_LIMBS); smaller NTT-sized products keep the reference's CPU
+# mul_fpntt2!/sqr_fpntt2!.  Measured with bench.py --route (route_crossover:
+# GPU call vs GMP on one core x the reference's published mul!/mpn_mul ratio).
+const GPU_MIN_LIMBS = Ref(4864)
+const GPU_MIN_SQR_LIMBS = Ref(4864)
+gpu_pays(m::Int, n::Int) = min(m, n) >= GPU_MIN_LIMBS[]
+gpu_pays_sqr(n::Int) = n >= GPU_MIN_SQR_LIMBS[]
+
+# Replaces the engine entry points of the enclosing NativeBigInt module so that
+# every NTT-sized mul!/sqr!/mul_bal! (src/mul.jl:134, :146, :161, :388-390) and
+# NBig * (src/nbig.jl:124-140) at or above the crossover runs on the GPU.  The
+# reference's own CPU methods stay reachable for the smaller products: they are
+# called in the world age captured before the replacement
+# (Base.invoke_in_world), so nothing of the CPU engine is copied.
+# min_limbs / min_sqr_limbs override the measured crossover (0: every product
+# on the GPU).
+function install!(mod::Module = parentmodule(@__MODULE__); min_limbs::Int = GPU_MIN_LIMBS[],
+                  min_sqr_limbs::Int = GPU_MIN_SQR_LIMBS[])
+    GPU_MIN_LIMBS[] = min_limbs
+    GPU_MIN_SQR_LIMBS[] = min_sqr_limbs
+    world = Base.get_world_counter()
+    cpu_mul = getfield(mod, :mul_fpntt2!)
+    cpu_sqr = getfield(mod, :sqr_fpntt2!)
     @eval mod begin
-        mul_fpntt2!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, m::Int, b::Memory{Limb}, bo::Int, n::Int) =
-            $(gpu_mul_fpntt2!)(r, ro, a, ao, m, b, bo, n)
-        sqr_fpntt2!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, n::Int) =
-            $(gpu_sqr_fpntt2!)(r, ro, a, ao, n)
+        function mul_fpntt2!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, m::Int, b::Memory{Limb}, bo::Int,
+                             n::Int)
+            if $(gpu_pays)(m, n)
+                return $(gpu_mul_fpntt2!)(r, ro, a, ao, m, b, bo, n)
+            end
+            return Base.invoke_in_world($world, $cpu_mul, r, ro, a, ao, m, b, bo, n)
+        end
+        function sqr_fpntt2!(r::Memory{Limb}, ro::Int, a::Memory{Limb}, ao::Int, n::Int)
+            if $(gpu_pays_sqr)(n)
+                return $(gpu_sqr_fpntt2!)(r, ro, a, ao, n)
+            end
+            return Base.invoke_in_world($world, $cpu_sqr, r, ro, a, ao, n)
+        end
     end
     return nothing
 end

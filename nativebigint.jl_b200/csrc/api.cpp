@@ -771,9 +771,8 @@ int nbg_unpack_dev(uint64_t* r, int64_t rn, const double* x1, const double* x2, 
     P.agg = (uint32_t*)(d + ao);
     CUDA_TRY(cudaMemcpyAsync(d, &P, sizeof P, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(d + jo, jobs.data(), sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, st));
-    const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / b + 4;
     CUDA_TRY(launch_jobs(JK_UNPACK, (const DProd*)d, E.d_plans, job_list((const Job*)(d + jo)), P.ntl,
-                         sizeof(uint64_t) * 2 * align_up((size_t)ncoef, 2), 0, st));
+                         unpack_smem_bytes(b), 0, st));
     CUDA_TRY(launch_jobs(JK_CARRY, (const DProd*)d, E.d_plans, job_list((const Job*)(d + jo) + P.ntl), 1, 0, 0, st));
     CUDA_TRY(launch_jobs(JK_CARRYFIX, (const DProd*)d, E.d_plans, job_list((const Job*)(d + jo)), P.ntl, 0, 0, st));
     g_launches += 3;

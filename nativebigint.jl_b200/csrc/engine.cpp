@@ -877,8 +877,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
             g.bytes += jobs * 2.0 * 16.0 * pts;
         }
     }
-    const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / bmin + 4;
-    const size_t unp_smem = sizeof(uint64_t) * 2 * (size_t)align_up((size_t)ncoef, 2);
+    const size_t unp_smem = unpack_smem_bytes(bmin);
     // unpack: product k owns tiles [agg_off[k], agg_off[k] + ntl); carry: one CTA per product
     Group& gu = group_of(2 * pmax - 1, JK_UNPACK, unp_smem);
     gu.mode = JM_TILES;

@@ -758,16 +758,9 @@ __device__ __forceinline__ void garner(const double* __restrict__ x1, const doub
     hi = phi + (lo < plo ? 1ULL : 0ULL);
 }
 
-// 64-bit slice of c * 2^d for d in [-127, 63]
-__device__ __forceinline__ uint64_t slice64(uint64_t lo, uint64_t hi, int d) {
-    if (d >= 0) return d == 0 ? lo : (lo << d);
-    int s = -d;
-    if (s >= 64) return s == 64 ? hi : (hi >> (s - 64));
-    return (lo >> s) | (hi << (64 - s));
-}
-
 constexpr int UNPACK_THREADS = 256;
 constexpr int LIMBS_PER_THREAD = UNPACK_TL / UNPACK_THREADS;
+static_assert(LIMBS_PER_THREAD == 4, "the limb window below is written for 4 limbs per thread");
 
 __device__ __forceinline__ uint32_t gp_compose(uint32_t lower, uint32_t upper) {
     // (g,p) pairs packed as bit0 = generate, bit1 = propagate; lower then upper.
@@ -776,120 +769,116 @@ __device__ __forceinline__ uint32_t gp_compose(uint32_t lower, uint32_t upper) {
     return g | (p << 1);
 }
 
-// floor(x / b) for 0 <= x < 2^50 and 1 <= b <= 52: a double quotient is off
-// by at most one, fixed by an exact integer check.
-__device__ __forceinline__ int64_t fdiv_small(int64_t x, int b, double rb) {
-    int64_t q = (int64_t)__dmul_rn((double)x, rb);
-    if (q * b > x) q--;
-    else if ((q + 1) * b <= x) q++;
-    return q;
+// 3-word window W += c * 2^d, c = (lo, hi) < 2^100, 0 <= d < 64 (the sum stays below 2^192)
+__device__ __forceinline__ void window_add(uint64_t& W0, uint64_t& W1, uint64_t& W2, uint64_t lo, uint64_t hi,
+                                           uint32_t d) {
+    const uint64_t a0 = lo << d;
+    const uint64_t a1 = ((lo >> 1) >> (63 - d)) | (hi << d);
+    const uint64_t a2 = (hi >> 1) >> (63 - d);
+    asm("add.cc.u64 %0, %0, %3;\n\t"
+        "addc.cc.u64 %1, %1, %4;\n\t"
+        "addc.u64 %2, %2, %5;"
+        : "+l"(W0), "+l"(W1), "+l"(W2)
+        : "l"(a0), "l"(a1), "l"(a2));
 }
 
-// Slices of the coefficients overlapping limb w, summed: returns the low 64
-// bits, sets hi (<= 4).  [i0, i1] is the coefficient range of the limb.
-__device__ __forceinline__ uint64_t limb_sum(const uint64_t* __restrict__ clo, const uint64_t* __restrict__ chi,
-                                             int64_t ibase, int64_t i0, int64_t i1, int b, int64_t w,
-                                             uint64_t& hiout) {
-    uint64_t lo = 0, hi = 0;
-    int d = (int)(i0 * b - 64 * w);
-    for (int64_t i = i0; i <= i1; i++, d += b) {
-        uint64_t sl = slice64(clo[i - ibase], chi[i - ibase], d);
-        lo += sl;
-        hi += (lo < sl) ? 1ULL : 0ULL;
+// Limbs [wt, wt + 4) of the sum of the coefficients i..iend (those that start
+// in bits [64 wt, 64 (wt + 4)); d = b i - 64 wt), streamed through a 3-word
+// window; the part above the range comes back as the spill (s0, s1), limbs
+// wt + 4 and wt + 5.  OWN = false keeps only the spill.
+template <bool OWN>
+__device__ __forceinline__ void range_limbs(const ulonglong2* __restrict__ cs, int64_t ibase, int64_t i, int64_t iend,
+                                            uint32_t d, uint32_t b, uint64_t* own, uint64_t& s0, uint64_t& s1) {
+    uint64_t W0 = 0, W1 = 0, W2 = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        while (i <= iend && d < 64) {
+            const ulonglong2 c = cs[i - ibase];
+            window_add(W0, W1, W2, c.x, c.y, d);
+            i++;
+            d += b;
+        }
+        if (OWN) own[q] = W0;
+        W0 = W1;
+        W1 = W2;
+        W2 = 0;
+        d -= 64;
     }
-    hiout = hi;
-    return lo;
+    s0 = W0;
+    s1 = W1;
 }
 
-// coefficient range [i0, i1] overlapping limb w, clamped to [ilo, ihi]
-__device__ __forceinline__ void limb_range(int64_t w, int b, double rb, int64_t ilo, int64_t ihi, int64_t& i0,
-                                           int64_t& i1) {
-    const int64_t a = 64 * w - 99;
-    i0 = a <= 0 ? 0 : fdiv_small(a + b - 1, b, rb);
-    i1 = fdiv_small(64 * w + 63, b, rb);
-    if (i0 < ilo) i0 = ilo;
-    if (i1 > ihi) i1 = ihi;
-}
-
-__global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restrict__ prods,
-                                                           const DPlan* __restrict__ plans,
-                                                           const Job* __restrict__ jobs, int64_t njobs) {
-    extern __shared__ uint64_t usm[];
+__global__ void __launch_bounds__(UNPACK_THREADS, 4) k_unpack(const DProd* __restrict__ prods,
+                                                              const DPlan* __restrict__ plans,
+                                                              const Job* __restrict__ jobs, int64_t njobs) {
+    extern __shared__ ulonglong2 ucs[];
     __shared__ uint32_t wagg[UNPACK_THREADS / 32];
-    __shared__ uint64_t hilast[UNPACK_THREADS + 1];
+    __shared__ uint64_t spill[UNPACK_THREADS + 1][2];
     for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
         const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int b = P.bch;
-        const double rb = 1.0 / (double)b;
         const int64_t N = pl.N;
         const int64_t w0 = jb.tile * UNPACK_TL;
         const int64_t w1 = min(w0 + (int64_t)UNPACK_TL, P.rn);
-        const int64_t wlo = w0 > 0 ? w0 - 1 : 0;
-        int64_t ilo = 64 * wlo - 99;
-        ilo = ilo <= 0 ? 0 : (ilo + b - 1) / b;
-        int64_t ihi = (64 * (w1 - 1) + 63) / b;
+        // coefficients that start in bits [64 (w0 - 4), 64 w1): the tile's own and
+        // those of the 4-limb range below it, whose spill reaches limb w0
+        const int64_t wlo = w0 >= 4 ? w0 - 4 : 0;
+        const int64_t ilo = (64 * wlo + b - 1) / b;
+        int64_t ihi = (64 * w1 - 1) / b;
         if (ihi > P.nconv - 1) ihi = P.nconv - 1;
         const int64_t ncoef = ihi >= ilo ? ihi - ilo + 1 : 0;
-        uint64_t* clo = usm;
-        uint64_t* chi = usm + ((ncoef + 1) & ~1LL);
         __syncthreads();
         for (int64_t k = threadIdx.x; k < ncoef; k += blockDim.x) {
-            int64_t i = ilo + k;
-            int64_t idx = i == 0 ? 0 : N - i;
+            const int64_t i = ilo + k;
+            const int64_t idx = i == 0 ? 0 : N - i;
             uint64_t lo, hi;
             garner(P.xa[0], P.xa[1], idx, pl, lo, hi);
-            clo[k] = lo;
-            chi[k] = hi;
+            ucs[k] = make_ulonglong2(lo, hi);
         }
         __syncthreads();
-        // limb sums for this thread's LIMBS_PER_THREAD consecutive limbs
         const int t = threadIdx.x;
-        uint64_t lo[LIMBS_PER_THREAD], hiv[LIMBS_PER_THREAD];
+        const int64_t wt = w0 + 4 * (int64_t)t;
+        uint64_t own[4], s0, s1;
         {
-            const int64_t wt = w0 + (int64_t)t * LIMBS_PER_THREAD;
-            int64_t i0, i1;
-            limb_range(wt, b, rb, ilo, ihi, i0, i1);
-#pragma unroll
-            for (int q = 0; q < LIMBS_PER_THREAD; q++) {
-                const int64_t w = wt + q;
-                if (q > 0) {  // advance the range by one limb (64 bits): a step or two
-                    const int64_t a = 64 * w - 99;
-                    while (i0 * b < a) i0++;
-                    if (i0 < ilo) i0 = ilo;
-                    while ((i1 + 1) * b <= 64 * w + 63 && i1 + 1 <= ihi) i1++;
-                }
-                if (w < w1) lo[q] = limb_sum(clo, chi, ilo, i0, i1, b, w, hiv[q]);
-                else { lo[q] = 0; hiv[q] = 0; }
-            }
+            const int64_t i0 = (64 * wt + b - 1) / b;
+            const int64_t i1 = min((64 * (wt + 4) - 1) / b, ihi);
+            range_limbs<true>(ucs, ilo, i0, i1, (uint32_t)(b * i0 - 64 * wt), (uint32_t)b, own, s0, s1);
         }
-        hilast[t + 1] = hiv[LIMBS_PER_THREAD - 1];
+        spill[t + 1][0] = s0;
+        spill[t + 1][1] = s1;
         if (t == 0) {
-            uint64_t h0 = 0;
-            if (w0 > 0) {
-                int64_t i0, i1;
-                limb_range(w0 - 1, b, rb, ilo, ihi, i0, i1);
-                (void)limb_sum(clo, chi, ilo, i0, i1, b, w0 - 1, h0);
+            uint64_t p0 = 0, p1 = 0;
+            if (w0 > 0) {  // the spill of the range [w0 - 4, w0) into limbs w0, w0 + 1
+                const int64_t i0 = ilo;
+                const int64_t i1 = min((64 * w0 - 1) / b, ihi);
+                range_limbs<false>(ucs, ilo, i0, i1, (uint32_t)(b * i0 - 64 * wlo), (uint32_t)b, nullptr, p0, p1);
             }
-            hilast[0] = h0;
+            spill[0][0] = p0;
+            spill[0][1] = p1;
         }
         __syncthreads();
-        // resolve the slice-sum overflow: t_w = lo_w + hi_{w-1} -> (lo', generate)
-        uint64_t hin = hilast[t];
-        uint32_t gpq[LIMBS_PER_THREAD];
-        uint32_t agg = 2u;  // identity: propagate, no generate
-#pragma unroll
-        for (int q = 0; q < LIMBS_PER_THREAD; q++) {
-            int64_t w = w0 + (int64_t)t * LIMBS_PER_THREAD + q;
-            uint64_t v = lo[q] + hin;
-            uint32_t g = v < hin ? 1u : 0u;
-            hin = hiv[q];
-            lo[q] = v;
-            uint32_t p = (v == ~0ULL) ? 1u : 0u;
-            gpq[q] = (w < w1) ? (g | (p << 1)) : 2u;
-            agg = gp_compose(agg, gpq[q]);
+        // own + the spill from below: a carry (0 or 1) out of the 4 limbs, then
+        // generate / propagate across threads
+        uint32_t gen;
+        {
+            const uint64_t a0 = spill[t][0], a1 = spill[t][1];
+            uint32_t c;
+            asm("add.cc.u64 %0, %0, %5;\n\t"
+                "addc.cc.u64 %1, %1, %6;\n\t"
+                "addc.cc.u64 %2, %2, %7;\n\t"
+                "addc.cc.u64 %3, %3, %7;\n\t"
+                "addc.u32 %4, %8, %8;"
+                : "+l"(own[0]), "+l"(own[1]), "+l"(own[2]), "+l"(own[3]), "=r"(c)
+                : "l"(a0), "l"(a1), "l"(0ULL), "r"(0u));
+            gen = c;
         }
+        // limbs past the product's end are zero and must not propagate
+        uint32_t prop = 1u;
+#pragma unroll
+        for (int q = 0; q < 4; q++) prop &= (wt + q < w1 && own[q] == ~0ULL) ? 1u : 0u;
+        const uint32_t agg = gen | (prop << 1);
         // block exclusive scan of agg (carry-in to each thread, tile carry-in 0)
         const int lane = t & 31, wid = t >> 5;
         uint32_t incl = agg;
@@ -905,13 +894,26 @@ __global__ void __launch_bounds__(UNPACK_THREADS) k_unpack(const DProd* __restri
         uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
         if (lane == 0) excl = 2u;
         excl = gp_compose(wpre, excl);
-        uint32_t cin = excl & 1u;  // tile carry-in assumed 0
+        const uint64_t cin = excl & 1u;  // tile carry-in assumed 0
+        asm("add.cc.u64 %0, %0, %4;\n\t"
+            "addc.cc.u64 %1, %1, %5;\n\t"
+            "addc.cc.u64 %2, %2, %5;\n\t"
+            "addc.u64 %3, %3, %5;"
+            : "+l"(own[0]), "+l"(own[1]), "+l"(own[2]), "+l"(own[3])
+            : "l"(cin), "l"(0ULL));
+        if (wt + 3 < w1) {
+            ulonglong2* dst = reinterpret_cast<ulonglong2*>(P.r + wt);
+            if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+                dst[0] = make_ulonglong2(own[0], own[1]);
+                dst[1] = make_ulonglong2(own[2], own[3]);
+            } else {
 #pragma unroll
-        for (int q = 0; q < LIMBS_PER_THREAD; q++) {
-            int64_t w = w0 + (int64_t)t * LIMBS_PER_THREAD + q;
-            uint64_t out = lo[q] + cin;
-            cin = (gpq[q] & 1u) | ((gpq[q] >> 1) & cin);
-            if (w < w1) P.r[w] = out;
+                for (int q = 0; q < 4; q++) P.r[wt + q] = own[q];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (wt + q < w1) P.r[wt + q] = own[q];
         }
         if (t == blockDim.x - 1 && P.agg) {
             uint32_t tot = 2u;
@@ -1087,7 +1089,7 @@ cudaError_t kernels_init(double p1, double p2) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
         if (e != cudaSuccess) return e;
     }
-    g_smem_optin.store(optin - 4096);  // headroom for the largest static allocation (k_unpack)
+    g_smem_optin.store(optin - 8192);  // headroom for the largest static allocation (k_unpack, 4.1 KB)
     return cudaSuccess;
 }
 

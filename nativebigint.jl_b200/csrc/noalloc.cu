@@ -311,10 +311,9 @@ extern "C" int nbg_mul_dev_noalloc(uint64_t* r, const uint64_t* a, int64_t m, co
         NA_TRY(fill(ps.ntiles, 1, 1, p));
         NA_TRY(run(JK_REV, ps.ntiles, 2 * tile));
     }
-    const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 2) + 100) / bch + 4;
     NA_TRY(fill(ntl, 1, 1, 0));
     const int64_t jo_unpack = jo;
-    NA_TRY(run(JK_UNPACK, ntl, sizeof(uint64_t) * 2 * (size_t)((ncoef + 1) & ~1LL)));
+    NA_TRY(run(JK_UNPACK, ntl, unpack_smem_bytes(bch)));
     if (ntl > 1) {
         NA_TRY(fill(1, 1, 1, 0));
         NA_TRY(run(JK_CARRY, 1, 0));

@@ -184,6 +184,12 @@ enum JobKind : int32_t {
 };
 
 constexpr int UNPACK_TL = 1024;  // output limbs per unpack tile
+// Dynamic shared memory of one unpack tile for chunk width b: (lo, hi) pairs of
+// the coefficients that start in bits [64 (w0 - 4), 64 (w0 + UNPACK_TL)).
+NBG_HD inline size_t unpack_smem_bytes(int b) {
+    const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 4)) / b + 2;
+    return 16 * (size_t)ncoef;
+}
 constexpr int PASS_THREADS = 256;
 
 // Shared-memory tiles are padded by one double every 16 so that strided

@@ -114,7 +114,8 @@ int nbg_batch_destroy(nbg_batch *bt);
 /* Per launch of a batch (up to cap): kernel kind (0 forward pass, 1 last pass
  * with pointwise product, 2 reverse pass, 3 unpack, 4 carry, 5 carries through
  * runs of all-ones limbs, 6 the last pass with one CTA per prime, 7 the last
- * pass of products with a kept operand spectrum), jobs, and the
+ * pass of products with a kept operand spectrum, 8 and 9 the forward and
+ * reverse column passes with tiles staged by TMA), jobs, and the
  * algorithmic FP64 instruction count and compulsory bytes of the reference
  * schedule for that launch.  Any output pointer may be NULL. */
 int nbg_batch_stats(const nbg_batch *bt, int32_t *kinds, int64_t *njobs, double *alg_ops, double *alg_bytes,
@@ -306,6 +307,12 @@ const char *nbg_last_error(void);
 void *nbg_default_stream(void);
 /* counters: kernel launches issued by this library since load */
 int64_t nbg_launch_count(void);
+/* Diagnostic, no counterpart in the reference: the number of bounded waits in
+ * the library's kernels (the TMA tile loads of the column passes wait on an
+ * mbarrier for at most about two seconds) that gave up on the current device
+ * since the last call, after which the kernel returned early and its results
+ * are invalid; reading clears the count.  Synchronizes the device. */
+int nbg_device_faults(int64_t *count);
 /* Diagnostic, no counterpart in the reference: the binary version (major * 10
  * + minor, cudaFuncGetAttributes) of the transform kernels as the CUDA runtime
  * loaded them on the current device, 100 for the sm_100a build; NBG_ECUDA

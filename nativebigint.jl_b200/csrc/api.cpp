@@ -205,7 +205,7 @@ int host_batch(const nbg_desc* descs, int64_t count) {
             }
             // descriptors and job table through the slot's pinned staging buffer
             if ((crc = E.ensure_stage(buf, c.bb.head_bytes))) break;
-            bind_batch(c.bb, base);
+            if ((crc = bind_batch(c.bb, base))) break;
             stage_batch(c.bb, E.stage[buf]);
             if (cudaMemcpyAsync(base, E.stage[buf], c.bb.head_bytes, cudaMemcpyHostToDevice, E.copy_in) != cudaSuccess) {
                 crc = fail(NBG_ECUDA, "descriptor copy failed");
@@ -483,6 +483,16 @@ void* nbg_default_stream(void) {
 
 int64_t nbg_launch_count(void) { return g_launches.load(); }
 
+int nbg_device_faults(int64_t* count) {
+    if (!count) return fail(NBG_EINVAL, "null pointer");
+    std::lock_guard<std::recursive_mutex> lk(g_eng.mu);
+    unsigned int n = 0;
+    cudaError_t e = kernels_take_faults(&n);
+    if (e != cudaSuccess) return fail(NBG_ECUDA, "reading the fault count: %s", cudaGetErrorString(e));
+    *count = (int64_t)n;
+    return NBG_OK;
+}
+
 int nbg_kernel_arch(int32_t* version) {
     if (!version) return fail(NBG_EINVAL, "null pointer");
     int v = 0;
@@ -668,7 +678,7 @@ int nbg_batch_profile(nbg_batch* bt, void* stream, float* ms, int32_t cap) {
     CUDA_TRY(cudaEventRecord(ev[0], st));
     for (size_t i = 0; i < ls.size(); i++) {
         const Launch& L = ls[i];
-        cudaError_t e = launch_jobs(L.kind, prods, g_eng.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st);
+        cudaError_t e = launch_jobs(L.kind, prods, g_eng.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st, L.odd);
         if (e != cudaSuccess) { rc = fail(NBG_ECUDA, "profile launch: %s", cudaGetErrorString(e)); break; }
         g_launches++;
         CUDA_TRY(cudaEventRecord(ev[i + 1], st));

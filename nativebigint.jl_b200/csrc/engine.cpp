@@ -23,6 +23,8 @@
 #include <tuple>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "../../include/nbgpu.h"
 #include "engine.h"
 #include "consts.h"
@@ -203,8 +205,8 @@ std::string Tuning::to_json() const {
     char buf[512];
     snprintf(buf, sizeof buf,
              "{\"full_max_mul\": %d, \"full_max_sqr\": %d, \"last_max\": %d, \"last_max_sqr\": %d, "
-             "\"early_gmax\": %d, \"tile_target\": %d, \"cmax\": %d, \"overrides\": [",
-             full_max_mul, full_max_sqr, last_max, last_max_sqr, early_gmax, tile_target, cmax);
+             "\"early_gmax\": %d, \"tile_target\": %d, \"cmax\": %d, \"tma\": %d, \"overrides\": [",
+             full_max_mul, full_max_sqr, last_max, last_max_sqr, early_gmax, tile_target, cmax, tma);
     std::string out = buf;
     bool first = true;
     for (const auto& kv : overrides) {
@@ -272,12 +274,14 @@ int Tuning::from_json(const char* js) {
     json_int(head.c_str(), "early_gmax", &t.early_gmax);
     json_int(head.c_str(), "tile_target", &t.tile_target);
     json_int(head.c_str(), "cmax", &t.cmax);
+    json_int(head.c_str(), "tma", &t.tma);
     auto pow2 = [](int v) { return v >= 1 && (v & (v - 1)) == 0; };
     // shared memory bounds: a product's last pass holds 4 tiles (a, b per
     // prime), a square's 2; column passes hold 2 tiles of <= tile_target or G.
     if (!pow2(t.cmax) || t.last_max < 4 || t.last_max_sqr < 4 || t.early_gmax < 2 || t.tile_target < 1 ||
         t.full_max_mul < 4 || t.full_max_sqr < 4 || t.full_max_mul > 4096 || t.full_max_sqr > 8192 ||
-        t.last_max > 4096 || t.last_max_sqr > 8192 || t.early_gmax > 1024 || t.tile_target > 8192)
+        t.last_max > 4096 || t.last_max_sqr > 8192 || t.early_gmax > 1024 || t.tile_target > 8192 ||
+        (t.tma != 0 && t.tma != 1))
         return fail(NBG_EINVAL, "tuning out of range");
     if (ov) {
         t.overrides.clear();
@@ -679,6 +683,47 @@ int Engine::ensure_pool(size_t bytes) {
 }
 
 // ---------------------------------------------------------------------------
+// TMA tensor maps (cuTensorMapEncodeTiled through the runtime's driver entry
+// point, so the library needs no link against libcuda)
+
+static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// A column pass's tiles can be staged by TMA: at least 16 and at most 256
+// columns (the dense shared-memory layout is free of bank conflicts from 16
+// columns on; a box edge holds at most 256 elements) and at most 256 rows.
+static bool tma_pass_ok(const DPass& ps) {
+    return ps.C >= 16 && ps.C <= 256 && ps.G <= 256 && ps.Qb % ps.C == 0 && tma_encoder() != nullptr;
+}
+
+// The 3-D map over nbuf transform buffers of N doubles at base: dims (Qb, N/Qb,
+// nbuf), box (C, G, 2): one box is one tile of both primes of one product.
+static int encode_pass_map(void* out, double* base, int64_t N, int64_t nbuf, const DPass& ps) {
+    auto enc = tma_encoder();
+    if (!enc) return fail(NBG_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t dims[3] = {(cuuint64_t)ps.Qb, (cuuint64_t)(N / ps.Qb), (cuuint64_t)nbuf};
+    const cuuint64_t strides[2] = {(cuuint64_t)ps.Qb * sizeof(double), (cuuint64_t)N * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)ps.C, (cuuint32_t)ps.G, 2};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box,
+                     estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(NBG_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return NBG_OK;
+}
+
+// ---------------------------------------------------------------------------
 // batch construction
 
 static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -726,25 +771,14 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         npass[(size_t)k] = P.npass;
         pmax = std::max(pmax, P.npass);
         bmin = std::min(bmin, bch);
-        xa_off[(size_t)k] = work;
-        work += 2 * (size_t)N;
         if (q.keep_b && (P.npass != 1 || P.sqr))
             return fail(NBG_EINVAL, "product %lld: a kept operand spectrum needs a one-pass product", (long long)k);
-        if ((P.npass > 1 && !P.sqr) || q.keep_b) {
-            xb_off[(size_t)k] = work;
-            work += 2 * (size_t)N;
-            if (q.keep_b) P.flags |= PF_BSAVE;
-        } else {
-            xb_off[(size_t)k] = SIZE_MAX;
-        }
+        if (q.keep_b) P.flags |= PF_BSAVE;
         agg_off[(size_t)k] = aggw;
         aggw += (size_t)P.ntl;
         bb.plan_of.push_back(pr);
     }
-    bb.work_doubles = work;
     bb.agg_words = aggw;
-    bb.xa_off = xa_off;
-    bb.xb_off = xb_off;
     bb.agg_off = agg_off;
 
     // Jobs of one pipeline step, grouped by kernel and shared-memory size: a
@@ -775,10 +809,15 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         int mode = JM_SEGS;
         double ops = 0, bytes = 0;
     };
-    // key: (step order, kind, smem)
-    std::map<std::tuple<int, int, size_t>, Group> groups;
-    auto group_of = [&](int order, int kind, size_t smem) -> Group& {
-        return groups[std::make_tuple(order, kind, smem)];
+    // key: (step order, kind, smem, odd stages present)
+    std::map<std::tuple<int, int, size_t, int>, Group> groups;
+    auto group_of = [&](int order, int kind, size_t smem, bool odd = false) -> Group& {
+        return groups[std::make_tuple(order, kind, smem, odd ? 1 : 0)];
+    };
+    auto pass_odd = [](const DPlan& pl, const DPass& ps) {
+        for (int st = ps.sa; st <= ps.sb; st++)
+            if (pl.st[st].m & 1) return true;
+        return false;
     };
     // step order: forward steps 0..pmax-2, the pointwise step pmax-1, reverse
     // steps pmax..2pmax-2, unpack 2pmax-1, carry 2pmax
@@ -798,6 +837,8 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         return (bb.prods[(size_t)x].flags & PF_BSAVE) < (bb.prods[(size_t)y].flags & PF_BSAVE);
     });
     std::vector<int32_t> cls;
+    bb.class_of.assign((size_t)count, -1);
+    const Tuning& tun = E.tun;
     // A batch whose last-pass tiles are fewer than one wave of CTAs (3 per SM)
     // gives each prime of a tile its own CTA: twice the CTAs, half the
     // critical path each (small batches are latency-bound).
@@ -822,6 +863,33 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         const int Pn = P0.npass;
         const int nop = P0.sqr ? 1 : 2;
         const double nc = (double)cls.size();
+        // the class's transform buffers are contiguous: [xa of each product][xb of each product]
+        {
+            const size_t N2 = 2 * (size_t)pl.N;
+            const bool has_b = (Pn > 1 && !P0.sqr) || keep0;
+            BatchBuild::ClassRec cr;
+            cr.xa0 = work;
+            cr.xb0 = has_b ? work + N2 * cls.size() : SIZE_MAX;
+            cr.nprod = (int32_t)cls.size();
+            cr.plan = bb.plan_of[(size_t)cls[0]];
+            for (size_t j = 0; j < cls.size(); j++) {
+                xa_off[(size_t)cls[j]] = cr.xa0 + N2 * j;
+                xb_off[(size_t)cls[j]] = has_b ? cr.xb0 + N2 * j : SIZE_MAX;
+                bb.prods[(size_t)cls[j]].tslot = (int32_t)j;
+            }
+            work += N2 * cls.size() * (has_b ? 2 : 1);
+            for (int p = 0; p < Pn - 1; p++) {
+                if (!tun.tma || !tma_pass_ok(pl.pass[p])) continue;
+                cr.tma_mask |= 1u << p;
+                if (cr.map0 < 0) {
+                    cr.map0 = bb.ntmaps;
+                    bb.ntmaps += 2 * (Pn - 1);
+                }
+            }
+            bb.classes.push_back(cr);
+            for (int32_t k : cls) bb.class_of[(size_t)k] = (int32_t)bb.classes.size() - 1;
+        }
+        const uint32_t tmask = bb.classes.back().tma_mask;
         auto emit = [&](Group& g, const DPass& ps, int nopnd, int sub_base) {
             JobSeg sg;
             const int64_t per = ps.Qb / ps.C, nblk = ps.ntiles / per;
@@ -840,10 +908,12 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         };
         for (int p = 0; p < Pn - 1; p++) {
             const DPass& ps = pl.pass[p];
-            const size_t smem = sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
+            const bool tp = (tmask >> p) & 1u;
+            const size_t smem = tp ? 128 + sizeof(double) * 2 * (size_t)(ps.G * ps.C)
+                                   : sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
             const double jobs = (double)ps.ntiles * nop * nc;
-            Group& g = group_of(pmax - Pn + p, JK_FWD, smem);
+            Group& g = group_of(pmax - Pn + p, tp ? JK_FWD_TMA : JK_FWD, smem, pass_odd(pl, ps));
             emit(g, ps, nop, p << 8);
             g.ops += jobs * 2.0 * pass_ops(pl, ps, true);
             // first pass reads packed limbs (bch bits per point), later ones both primes' doubles
@@ -860,7 +930,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
                                 (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
             const double jobs = (double)ps.ntiles * nc;  // tiles of both primes (the work, split or not)
-            Group& g = group_of(pmax - 1, keep ? JK_PWR_KEEP : split ? JK_PWR_SPLIT : JK_PWR, smem);
+            Group& g = group_of(pmax - 1, keep ? JK_PWR_KEEP : split ? JK_PWR_SPLIT : JK_PWR, smem, pass_odd(pl, ps));
             emit(g, ps, split ? 2 : 1, (Pn - 1) << 8);  // split: "operand" is the prime
             g.ops += jobs * 2.0 * (nop * pass_ops(pl, ps, true) + 7.0 * pts + pass_ops(pl, ps, false));
             const double in_b = Pn == 1 ? (double)ps.ntiles * nop * pts * sum_bch / 8.0 : jobs * 2.0 * nop * 8.0 * pts;
@@ -868,15 +938,20 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         }
         for (int p = Pn - 2; p >= 0; p--) {
             const DPass& ps = pl.pass[p];
-            const size_t smem = sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
+            const bool tp = (tmask >> p) & 1u;
+            const size_t smem = tp ? 128 + sizeof(double) * 2 * (size_t)(ps.G * ps.C)
+                                   : sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
             const double jobs = (double)ps.ntiles * nc;
-            Group& g = group_of(pmax + (Pn - 2 - p), JK_REV, smem);
+            Group& g = group_of(pmax + (Pn - 2 - p), tp ? JK_REV_TMA : JK_REV, smem, pass_odd(pl, ps));
             emit(g, ps, 1, p << 8);
             g.ops += jobs * 2.0 * pass_ops(pl, ps, false);
             g.bytes += jobs * 2.0 * 16.0 * pts;
         }
     }
+    bb.work_doubles = work;
+    bb.xa_off = xa_off;
+    bb.xb_off = xb_off;
     const size_t unp_smem = unpack_smem_bytes(bmin);
     // unpack: product k owns tiles [agg_off[k], agg_off[k] + ntl); carry: one CTA per product
     Group& gu = group_of(2 * pmax - 1, JK_UNPACK, unp_smem);
@@ -908,6 +983,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         const Group& g = kv.second;
         const int kind = std::get<1>(kv.first);
         Launch L{kind, bb.total_jobs, g.njobs, std::get<2>(kv.first)};
+        L.odd = std::get<3>(kv.first) != 0;
         bb.total_jobs += g.njobs;
         L.step = std::get<0>(kv.first);
         L.alg_ops = g.ops;
@@ -924,7 +1000,9 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         bb.launches.push_back(L);
     }
     bb.tstart_off = tb;
-    tb = align_up(tb + sizeof(int64_t) * ((size_t)count + 1), 16);
+    tb = align_up(tb + sizeof(int64_t) * ((size_t)count + 1), 128);
+    bb.tmap_off = tb;  // 128-byte tensor maps, written by bind_batch
+    tb = align_up(tb + 128 * (size_t)bb.ntmaps, 16);
     bb.expand_off = tb;
     tb = align_up(tb + sizeof(ExpandEntry) * bb.launches.size(), 16);
     bb.table.assign(tb, 0);
@@ -953,9 +1031,24 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
     return NBG_OK;
 }
 
-void bind_batch(BatchBuild& bb, char* dbase) {
+int bind_batch(BatchBuild& bb, char* dbase) {
     double* work = (double*)(dbase + bb.off_work);
     uint32_t* agg = (uint32_t*)(dbase + bb.off_agg);
+    // tensor maps of the TMA column passes, per class [pass][operand]
+    for (const BatchBuild::ClassRec& cr : bb.classes) {
+        if (cr.map0 < 0) continue;
+        const DPlan& pl = cr.plan->d;
+        for (int p = 0; p + 1 < pl.npass; p++) {
+            if (!((cr.tma_mask >> p) & 1u)) continue;
+            for (int op = 0; op < 2; op++) {
+                const size_t off = op ? cr.xb0 : cr.xa0;
+                if (off == SIZE_MAX) continue;
+                char* dst = bb.table.data() + bb.tmap_off + 128 * (size_t)(cr.map0 + 2 * p + op);
+                int rc = encode_pass_map(dst, work + off, pl.N, 2 * (int64_t)cr.nprod, pl.pass[p]);
+                if (rc) return rc;
+            }
+        }
+    }
     for (size_t k = 0; k < bb.prods.size(); k++) {
         DProd& P = bb.prods[k];
         const int64_t N = bb.plan_of[k]->d.N;
@@ -968,6 +1061,8 @@ void bind_batch(BatchBuild& bb, char* dbase) {
             P.xb[0] = P.xb[1] = nullptr;
         }
         P.agg = agg + bb.agg_off[k];
+        const BatchBuild::ClassRec& cr = bb.classes[(size_t)bb.class_of[k]];
+        P.tmap = cr.map0 < 0 ? nullptr : dbase + bb.off_jobs + bb.tmap_off + 128 * (size_t)cr.map0;
     }
     ExpandEntry* ex = (ExpandEntry*)(bb.table.data() + bb.expand_off);
     for (size_t i = 0; i < bb.launches.size(); i++) {
@@ -975,6 +1070,7 @@ void bind_batch(BatchBuild& bb, char* dbase) {
         ex[i].begin = bb.launches[i].off;
         ex[i].n = bb.launches[i].n;
     }
+    return NBG_OK;
 }
 
 void stage_batch(const BatchBuild& bb, char* host) {
@@ -997,7 +1093,8 @@ JobSrc launch_src(const BatchBuild& bb, const Launch& L, const char* dbase) {
 
 // Point the descriptors at the device block and upload descriptors + job table.
 int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st) {
-    bind_batch(bb, dbase);
+    int rc = bind_batch(bb, dbase);
+    if (rc) return rc;
     CUDA_TRY(cudaMemcpyAsync(dbase + bb.off_prods, bb.prods.data(), sizeof(DProd) * bb.prods.size(),
                              cudaMemcpyHostToDevice, st));
     if (!bb.table.empty())
@@ -1020,7 +1117,7 @@ int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, 
         g_launches++;
     }
     for (const Launch& L : bb.launches) {
-        cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st);
+        cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st, L.odd);
         if (e != cudaSuccess) return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n,
                                           cudaGetErrorString(e));
         g_launches++;
@@ -1052,7 +1149,7 @@ int run_launches_branched(Engine& E, const BatchBuild& bb, char* dbase, cudaStre
                 s = side[(k - i - 1) % (size_t)nside];
                 CUDA_TRY(cudaStreamWaitEvent(s, fork, 0));
             }
-            cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, s);
+            cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, s, L.odd);
             if (e != cudaSuccess)
                 return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n, cudaGetErrorString(e));
             g_launches++;

@@ -38,6 +38,7 @@ struct Tuning {
     int early_gmax = 256;     // largest row count of an early (column) pass
     int tile_target = 2048;   // target doubles per column-pass tile
     int cmax = 128;           // most adjacent columns per column-pass tile
+    int tma = 1;              // stage column tiles of at least 16 columns by TMA (0: cp.async for all)
     std::map<int64_t, SplitOverride> overrides;  // key: N * 2 + square
     std::string to_json() const;
     int from_json(const char* js);
@@ -110,6 +111,7 @@ struct Launch {
     int nseg = 0;
     size_t seg_off = 0, plist_off = 0;
     int step = 0;          // pipeline step: launches of one step are independent
+    bool odd = true;       // some pass of the launch holds a radix-3/5/7 stage
     double alg_ops = 0;    // FP64 instructions of the reference schedule done by this launch
     double alg_bytes = 0;  // compulsory global bytes (operand/limb reads, tile loads and stores)
 };
@@ -125,6 +127,19 @@ struct BatchBuild {
     size_t head_bytes = 0;    // [0, head_bytes): descriptors and table, the host-written head
     std::vector<Launch> launches;
     std::vector<size_t> xa_off, xb_off, agg_off;
+    // product classes (one plan, one kept-spectrum flag): contiguous transform
+    // buffers, and the tensor maps of their TMA column passes
+    struct ClassRec {
+        size_t xa0 = 0, xb0 = 0;  // first buffers (doubles into the workspace); xb0 SIZE_MAX: none
+        int32_t nprod = 0;
+        int32_t map0 = -1;        // first of 2 * (passes - 1) tensor maps ([pass][operand]); -1: none
+        uint32_t tma_mask = 0;    // column passes staged by TMA
+        const PlanRec* plan = nullptr;
+    };
+    std::vector<ClassRec> classes;
+    std::vector<int32_t> class_of;  // per product
+    size_t tmap_off = 0;            // tensor maps in the table (128 B each)
+    int ntmaps = 0;
     size_t work_doubles = 0, agg_words = 0;
     size_t off_prods = 0, off_jobs = 0, off_work = 0, off_agg = 0, dev_bytes = 0;
 };
@@ -132,8 +147,9 @@ struct BatchBuild {
 int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb);
 int upload_batch(Engine& E, BatchBuild& bb, char* dbase, cudaStream_t st);
 // Points each product's workspace and carry words into the batch's device
-// region at dbase (what upload_batch does before copying).
-void bind_batch(BatchBuild& bb, char* dbase);
+// region at dbase and encodes the TMA tensor maps over it (what upload_batch
+// does before copying).
+int bind_batch(BatchBuild& bb, char* dbase);
 // Writes the bound descriptors and job table into `host` in their device
 // layout: head_bytes that one copy to dbase makes the region's head.
 void stage_batch(const BatchBuild& bb, char* host);

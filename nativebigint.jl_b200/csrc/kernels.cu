@@ -38,6 +38,7 @@
 #endif
 // Column passes with tile sets up to this size run the 4-CTA/SM build.
 constexpr size_t COL4_MAX_SMEM = 32 * 1024;
+constexpr size_t COL4_MAX_SMEM_TMA = 32 * 1024 + 128;  // the TMA tiles plus their mbarrier line
 // Rounds are inlined into the kernels; out-of-line rounds (NBG_ROUND_NOINLINE)
 // measured 40% slower in k_pwr.
 #ifdef NBG_ROUND_NOINLINE
@@ -54,6 +55,12 @@ __constant__ double c_garner[2];  // g = p1^-1 mod p2 (canonical) and g/p2
 __device__ __forceinline__ Fp fpctx(int f) { return c_fp[f]; }
 
 __device__ __forceinline__ int sp(int i) { return tile_pad_index(i); }
+// tile layouts: padded (one double in 16, the cp.async tiles) or dense (the
+// boxes TMA writes; column tiles with at least 16 columns, conflict-free)
+template <bool PAD>
+__device__ __forceinline__ int lay(int i) {
+    return PAD ? tile_pad_index(i) : i;
+}
 
 // exact double of an integer below 2^52: OR it into 2^52's mantissa, subtract 2^52
 __device__ __forceinline__ double small_u64_to_double(uint64_t c) {
@@ -102,7 +109,7 @@ __device__ __forceinline__ int split_unit(int u, int per, int& tau) {
 }
 
 // Generic stage: one butterfly per unit, any radix (odd stages, lone radix-4/2).
-template <int M, bool FWD>
+template <int M, bool FWD, bool PAD>
 __device__ NBG_ROUND void round_gen(const Tiles& T, const DStage& st) {
     const int C = 1 << T.lc;
     const int Lloc = (int)(st.L / T.Qb), Qloc = (int)(st.Q / T.Qb);
@@ -132,7 +139,7 @@ __device__ NBG_ROUND void round_gen(const Tiles& T, const DStage& st) {
         const int base = ((blk * Lloc + jl) << T.lc) + c;
         double y[M];
 #pragma unroll
-        for (int t = 0; t < M; t++) y[t] = s[sp(base + t * stride)];
+        for (int t = 0; t < M; t++) y[t] = s[lay<PAD>(base + t * stride)];
         if constexpr (M == 2) {
             butterfly2(y[0], y[1], F);
         } else {
@@ -150,7 +157,7 @@ __device__ NBG_ROUND void round_gen(const Tiles& T, const DStage& st) {
             butterfly<M, FWD>(y, w, rot, F);
         }
 #pragma unroll
-        for (int t = 0; t < M; t++) s[sp(base + t * stride)] = y[t];
+        for (int t = 0; t < M; t++) s[lay<PAD>(base + t * stride)] = y[t];
     }
 }
 
@@ -158,7 +165,7 @@ __device__ NBG_ROUND void round_gen(const Tiles& T, const DStage& st) {
 // (block b, j2 < L/16 rows, column c) holds rows b*L + j2 + t1*L/4 + t2*L/16.
 // Forward: A's butterflies run over t1 for each t2 (column j2 + t2*L/16), then
 // B's over t2 for each t1 (column j2).  Reverse: B then A, transposed.
-template <bool FWD>
+template <bool FWD, bool PAD>
 __device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStage& B) {
     const int C = 1 << T.lc;
     const int Lloc = (int)(A.L / T.Qb);
@@ -183,7 +190,7 @@ __device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStag
 #pragma unroll
         for (int t1 = 0; t1 < 4; t1++)
 #pragma unroll
-            for (int t2 = 0; t2 < 4; t2++) v[t1 * 4 + t2] = s[sp(((row0 + t1 * 4 * q16 + t2 * q16) << T.lc) + c)];
+            for (int t2 = 0; t2 < 4; t2++) v[t1 * 4 + t2] = s[lay<PAD>(((row0 + t1 * 4 * q16 + t2 * q16) << T.lc) + c)];
         const int jB = j2 * T.Qb + T.j0 + c;
         const double* twB = (p1 ? twB1 : twB0) + jB;
         const double* twA = (p1 ? twA1 : twA0) + jB;  // A's column for t2 is jB + t2*q16*Qb
@@ -216,7 +223,7 @@ __device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStag
 #pragma unroll
         for (int t1 = 0; t1 < 4; t1++)
 #pragma unroll
-            for (int t2 = 0; t2 < 4; t2++) s[sp(((row0 + t1 * 4 * q16 + t2 * q16) << T.lc) + c)] = v[t1 * 4 + t2];
+            for (int t2 = 0; t2 < 4; t2++) s[lay<PAD>(((row0 + t1 * 4 * q16 + t2 * q16) << T.lc) + c)] = v[t1 * 4 + t2];
     }
 }
 
@@ -421,29 +428,38 @@ __device__ NBG_ROUND void fused_r8(const FuseTiles& T, const DStage& A) {
     }
 }
 
-template <bool FWD>
+// PAD = false (dense TMA tiles) occurs only in column passes, which hold no
+// radix-8 or radix-2 round (those stages end a transform: the last pass).
+// ODD = false: the pass holds no radix-3/5/7 stage (every pass but the first of
+// an odd-length transform), so that code and its registers are left out.
+template <bool FWD, bool PAD = true, bool ODD = true>
 __device__ void run_round(const Tiles& T, const DPlan& pl, int kind, int s0) {
     __syncthreads();
     const DStage& st = pl.st[s0];
     switch (kind) {
-        case RK_R16: round_r16<FWD>(T, st, pl.st[s0 + 1]); break;
-        case RK_R8: round_r8<FWD>(T, st); break;
-        case RK_R4: round_gen<4, FWD>(T, st); break;
-        case RK_R2: round_gen<2, FWD>(T, st); break;
+        case RK_R16: round_r16<FWD, PAD>(T, st, pl.st[s0 + 1]); break;
+        case RK_R4: round_gen<4, FWD, PAD>(T, st); break;
+        case RK_R8:
+            if (PAD) round_r8<FWD>(T, st);
+            break;
+        case RK_R2:
+            if (PAD) round_gen<2, FWD, PAD>(T, st);
+            break;
         default:
-            if (st.m == 3) round_gen<3, FWD>(T, st);
-            else if (st.m == 5) round_gen<5, FWD>(T, st);
-            else round_gen<7, FWD>(T, st);
+            if (!ODD) break;
+            if (st.m == 3) round_gen<3, FWD, PAD>(T, st);
+            else if (st.m == 5) round_gen<5, FWD, PAD>(T, st);
+            else round_gen<7, FWD, PAD>(T, st);
             break;
     }
 }
 
-template <bool FWD>
+template <bool FWD, bool PAD = true, bool ODD = true>
 __device__ void run_pass(const Tiles& T, const DPlan& pl, const DPass& ps) {
     if (FWD) {
-        for (int r = 0; r < ps.nrounds; r++) run_round<true>(T, pl, ps.rkind[r], ps.rstage[r]);
+        for (int r = 0; r < ps.nrounds; r++) run_round<true, PAD, ODD>(T, pl, ps.rkind[r], ps.rstage[r]);
     } else {
-        for (int r = ps.nrounds - 1; r >= 0; r--) run_round<false>(T, pl, ps.rkind[r], ps.rstage[r]);
+        for (int r = ps.nrounds - 1; r >= 0; r--) run_round<false, PAD, ODD>(T, pl, ps.rkind[r], ps.rstage[r]);
     }
     __syncthreads();
 }
@@ -499,8 +515,9 @@ __device__ __forceinline__ void store_tile(const double* s, double* __restrict__
 }
 // one packed chunk written to both primes' tiles s0 and s1; chunks are
 // processed 4 per thread at a time so their limb loads overlap
+template <bool PAD = true>
 __device__ __forceinline__ void pack_tile2(double* s0, double* s1, const uint64_t* __restrict__ limbs, int64_t n,
-                                           int b, int64_t nch, const DPass& ps, int base) {
+                                           int b, int64_t nch, const DPass& ps, int64_t base) {
     const int lc = __ffs(ps.C) - 1;
     const int cnt = ps.G << lc;
     const int Qb = (int)ps.Qb;
@@ -528,8 +545,8 @@ __device__ __forceinline__ void pack_tile2(double* s0, double* s1, const uint64_
             uint64_t c = lo[q] >> sh[q];
             if (sh[q]) c |= hi[q] << (64 - sh[q]);
             const double v = live[q] ? small_u64_to_double(c & mask) : 0.0;
-            s0[sp(e)] = v;
-            s1[sp(e)] = v;
+            s0[lay<PAD>(e)] = v;
+            s1[lay<PAD>(e)] = v;
         }
     }
 }
@@ -552,7 +569,7 @@ __device__ __forceinline__ Tiles make_tiles(double* s, int stride, int ntiles, i
 // Forward pass of one tile of one operand, both primes (tiles X0, X1).
 // MINB: CTAs per SM the register budget is cut for (3: 80 registers, 4: 64);
 // launches pick 4 when the tile set is small enough for four CTAs' shared memory.
-template <int MINB>
+template <int MINB, bool ODD>
 __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const Job* __restrict__ jobs, int64_t njobs) {
@@ -583,7 +600,7 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restr
             load_tile_async(s1, x1, ps, base);
             cp_async_wait_all();
         }
-        run_pass<true>(make_tiles(smem, stride, 2, 0, ps, j0), pl, ps);
+        run_pass<true, true, ODD>(make_tiles(smem, stride, 2, 0, ps, j0), pl, ps);
         store_tile(s0, x0, ps, base);
         store_tile(s1, x1, ps, base);
     }
@@ -594,7 +611,7 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restr
 // SPLIT: one CTA per prime (JK_PWR_SPLIT).  KEEPB: launches of products with
 // a kept operand spectrum (JK_PWR_KEEP; PF_BSAVE / PF_BSPEC), compiled apart
 // so the other launches carry none of that code.
-template <bool SPLIT, bool KEEPB>
+template <bool SPLIT, bool KEEPB, bool ODD>
 __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const Job* __restrict__ jobs, int64_t njobs) {
@@ -652,7 +669,7 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
         const int lastk = ps.rkind[nr - 1];
         if (lastk == RK_R16 || lastk == RK_R8) {
             // forward rounds but the last, fused round, reverse rounds but the first
-            for (int r = 0; r < nr - 1; r++) run_round<true>(TF, pl, ps.rkind[r], ps.rstage[r]);
+            for (int r = 0; r < nr - 1; r++) run_round<true, true, ODD>(TF, pl, ps.rkind[r], ps.rstage[r]);
             __syncthreads();
             FuseTiles FT;
             FT.s = smem;
@@ -673,10 +690,10 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
                 store_tile(b0, P.xb[p0], ps, base);
                 if (pf < 0) store_tile(b1, P.xb[1], ps, base);
             }
-            for (int r = nr - 2; r >= 0; r--) run_round<false>(TR, pl, ps.rkind[r], ps.rstage[r]);
+            for (int r = nr - 2; r >= 0; r--) run_round<false, true, ODD>(TR, pl, ps.rkind[r], ps.rstage[r]);
             __syncthreads();
         } else {
-            run_pass<true>(TF, pl, ps);
+            run_pass<true, true, ODD>(TF, pl, ps);
             if (bsave) {
                 store_tile(b0, P.xb[p0], ps, base);
                 if (pf < 0) store_tile(b1, P.xb[1], ps, base);
@@ -695,7 +712,7 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
                     a0[i] = fp_mulmod(a0[i], b0[i], F);
                 }
             }
-            run_pass<false>(TR, pl, ps);
+            run_pass<false, true, ODD>(TR, pl, ps);
         }
         store_tile(a0, P.xa[p0], ps, base);
         if (pf < 0) store_tile(a1, P.xa[1], ps, base);
@@ -703,7 +720,7 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
 }
 
 // Reverse pass of one tile, both primes.
-template <int MINB>
+template <int MINB, bool ODD>
 __global__ void __launch_bounds__(PASS_THREADS, MINB) k_rev(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const Job* __restrict__ jobs, int64_t njobs) {
@@ -725,10 +742,147 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_rev(const DProd* __restr
         load_tile_async(smem, P.xa[0], ps, base);
         load_tile_async(smem + stride, P.xa[1], ps, base);
         cp_async_wait_all();
-        run_pass<false>(make_tiles(smem, stride, 2, 0, ps, j0), pl, ps);
+        run_pass<false, true, ODD>(make_tiles(smem, stride, 2, 0, ps, j0), pl, ps);
         store_tile(smem, P.xa[0], ps, base);
         store_tile(smem + stride, P.xa[1], ps, base);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Column passes staged by TMA.  The tiles of one (product class, pass,
+// operand) are boxes of one 3-D tensor map over the class's transform
+// buffers: x = column (Qb wide rows), y = row (N / Qb rows), z = buffer
+// (2 per product: prime 0, prime 1).  One cp.async.bulk.tensor load brings both
+// primes' G x C tiles into shared memory (dense, [prime][row][column]) and one
+// store writes them back; tiles have at least 16 columns, so the rounds' accesses
+// are free of bank conflicts without padding.  The tensor maps cover this GPU's
+// own workspace only, and no load uses cluster multicast.
+
+// mbarrier waits that gave up (the host reads and clears it: nbg_device_faults)
+__device__ unsigned int g_nbg_faults = 0;
+
+namespace tma {
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bar_expect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_try(uint64_t* bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(saddr(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the barrier's phase with a bound of about 2^32 SM clocks (two
+// seconds); returns false (and counts a fault) when it gives up.
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t phase) {
+    if (bar_try(bar, phase)) return true;
+    const long long t0 = clock64();
+    while (!bar_try(bar, phase)) {
+        if (clock64() - t0 > (1LL << 32)) {
+            if (threadIdx.x == 0) atomicAdd(&g_nbg_faults, 1u);
+            return false;
+        }
+    }
+    return true;
+}
+__device__ __forceinline__ void load3(void* dst, const void* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(saddr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(saddr(bar))
+        : "memory");
+}
+__device__ __forceinline__ void store3(const void* map, int x, int y, int z, const void* src) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];"
+                 ::"l"(map), "r"(x), "r"(y), "r"(z), "r"(saddr(src))
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// the bulk stores issued so far have read their shared-memory source
+__device__ __forceinline__ void stores_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// the bulk stores issued so far are complete
+__device__ __forceinline__ void stores_done() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// generic-proxy shared-memory accesses before this point are ordered before later async-proxy ones
+__device__ __forceinline__ void fence_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// a tensor map the host wrote to global memory, made visible to the tensor-map proxy
+__device__ __forceinline__ void fence_map(const void* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+}  // namespace tma
+
+// box origin of column tile t: x = first column, y = first row
+__device__ __forceinline__ void tile_box(const DPass& ps, int64_t t, int& x, int& y) {
+    const int64_t per = ps.Qb / ps.C;
+    const int64_t blk = t / per;
+    x = (int)((t - blk * per) * ps.C);
+    y = (int)(blk * ps.G);
+}
+
+// One column pass (forward or reverse) of one tile of one operand, both primes,
+// staged by TMA.  Dynamic shared memory: [mbarrier | 120 B | tiles].
+template <int MINB, bool FWD, bool ODD>
+__global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __restrict__ prods,
+                                                             const DPlan* __restrict__ plans,
+                                                             const Job* __restrict__ jobs, int64_t njobs) {
+    extern __shared__ __align__(128) double dsm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm);
+    double* smem = dsm + 16;  // tiles start 128 bytes in
+    if (threadIdx.x == 0) tma::bar_init(bar);
+    __syncthreads();
+    uint32_t phase = 0;
+    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
+    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
+    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
+        const Job jb = jobs[ji];
+        const DProd& P = prods[jb.prod];
+        const DPlan& pl = plans[P.plan];
+        const int opb = FWD ? (jb.sub >> 1) & 1 : 0;
+        const int pass = (jb.sub >> 8) & 0xff;
+        const DPass& ps = pl.pass[pass];
+        int x, y;
+        tile_box(ps, jb.tile, x, y);
+        const int z = 2 * P.tslot;
+        const void* map = static_cast<const char*>(P.tmap) + 128 * (2 * pass + opb);
+        const int cnt = ps.G * ps.C;
+        const bool pack = FWD && pass == 0 && !(P.flags & PF_PRELOADED);
+        __syncthreads();  // every thread is done with the previous tile
+        if (threadIdx.x == 0) {
+            tma::stores_read();  // the previous tile's store has read shared memory
+            if (!pack) {
+                tma::fence_map(map);
+                tma::bar_expect(bar, (uint32_t)(2 * cnt * sizeof(double)));
+                tma::load3(smem, map, x, y, z, bar);
+            }
+        }
+        if (pack) {
+            __syncthreads();
+            const int64_t base = (int64_t)(y / ps.G) * pl.st[ps.sa].L + x;
+            if (opb) pack_tile2<false>(smem, smem + cnt, P.b, P.n, P.bch, P.ncb, ps, base);
+            else pack_tile2<false>(smem, smem + cnt, P.a, P.m, P.bch, P.nca, ps, base);
+        } else {
+            if (!tma::bar_wait(bar, phase)) {  // gave up: leave after the stores issued so far
+                if (threadIdx.x == 0) tma::stores_done();
+                return;
+            }
+            phase ^= 1u;
+        }
+        run_pass<FWD, false, ODD>(make_tiles(smem, cnt, 2, 0, ps, x), pl, ps);
+        tma::fence_async();
+        __syncthreads();
+        if (threadIdx.x == 0) tma::store3(map, x, y, z, smem);
+    }
+    if (threadIdx.x == 0) tma::stores_done();
 }
 
 // ---------------------------------------------------------------------------
@@ -1079,9 +1233,17 @@ cudaError_t kernels_init(double p1, double p2) {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const void* ks[] = {(const void*)k_fwd<3>, (const void*)k_fwd<4>, (const void*)k_pwr<false, false>, (const void*)k_pwr<true, false>,
-                        (const void*)k_pwr<false, true>,
-                        (const void*)k_rev<3>, (const void*)k_rev<4>, (const void*)k_unpack};
+    const void* ks[] = {(const void*)k_fwd<3, true>, (const void*)k_fwd<4, true>, (const void*)k_fwd<3, false>,
+                        (const void*)k_fwd<4, false>,
+                        (const void*)k_pwr<false, false, true>, (const void*)k_pwr<true, false, true>,
+                        (const void*)k_pwr<false, true, true>, (const void*)k_pwr<false, false, false>,
+                        (const void*)k_pwr<true, false, false>, (const void*)k_pwr<false, true, false>,
+                        (const void*)k_rev<3, true>, (const void*)k_rev<4, true>, (const void*)k_rev<3, false>,
+                        (const void*)k_rev<4, false>, (const void*)k_unpack,
+                        (const void*)k_col_tma<3, true, true>, (const void*)k_col_tma<4, true, true>,
+                        (const void*)k_col_tma<3, false, true>, (const void*)k_col_tma<4, false, true>,
+                        (const void*)k_col_tma<3, true, false>, (const void*)k_col_tma<4, true, false>,
+                        (const void*)k_col_tma<3, false, false>, (const void*)k_col_tma<4, false, false>};
     for (const void* k : ks) {
         cudaFuncAttributes fa;
         e = cudaFuncGetAttributes(&fa, k);
@@ -1095,22 +1257,29 @@ cudaError_t kernels_init(double p1, double p2) {
 
 int kernels_smem_optin() { return g_smem_optin.load(); }
 
+cudaError_t kernels_take_faults(unsigned int* n) {
+    unsigned int zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(n, g_nbg_faults, sizeof(unsigned int));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(g_nbg_faults, &zero, sizeof zero);
+}
+
 cudaError_t kernels_binary_version(int* version) {
     cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)k_pwr<false, false>);
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)k_pwr<false, false, false>);
     if (e != cudaSuccess) return e;
     *version = fa.binaryVersion;
     return cudaSuccess;
 }
 
 cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& src, int64_t njobs,
-                        size_t smem, int grid_cap, cudaStream_t st) {
+                        size_t smem, int grid_cap, cudaStream_t st, bool odd) {
     // the kernels read an explicit job list (batches expand theirs on the device first)
     if (src.mode != JM_LIST) return cudaErrorInvalidValue;
     const Job* jobs = src.list;
     if (njobs <= 0) return cudaSuccess;
     int64_t grid64 = njobs;
-    if (kind == JK_FWD || kind == JK_REV) {
+    if (kind == JK_FWD || kind == JK_REV || kind == JK_FWD_TMA || kind == JK_REV_TMA) {
         // up to 8 consecutive jobs per CTA while keeping >= 4 waves of 3 CTAs per SM
         const int64_t k = std::max<int64_t>(1, std::min<int64_t>(8, njobs / (148 * 3 * 4)));
         grid64 = (njobs + k - 1) / k;
@@ -1118,17 +1287,31 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
     if (grid_cap > 0 && grid64 > grid_cap) grid64 = grid_cap;
     if (grid64 > 0x7fffffff) grid64 = 0x7fffffff;
     const unsigned grid = (unsigned)grid64;
+#define NBG_ODD(KERNEL, ...)                                                                      \
+    do {                                                                                          \
+        if (odd) KERNEL<__VA_ARGS__, true><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);   \
+        else KERNEL<__VA_ARGS__, false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);      \
+    } while (0)
+    const bool c4 = smem <= COL4_MAX_SMEM, c4t = smem <= COL4_MAX_SMEM_TMA;
     switch (kind) {
         case JK_FWD:
-            if (smem <= COL4_MAX_SMEM) k_fwd<4><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
-            else k_fwd<3><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
+            if (c4) NBG_ODD(k_fwd, 4);
+            else NBG_ODD(k_fwd, 3);
             break;
-        case JK_PWR: k_pwr<false, false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
-        case JK_PWR_SPLIT: k_pwr<true, false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
-        case JK_PWR_KEEP: k_pwr<false, true><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_FWD_TMA:
+            if (c4t) NBG_ODD(k_col_tma, 4, true);
+            else NBG_ODD(k_col_tma, 3, true);
+            break;
+        case JK_REV_TMA:
+            if (c4t) NBG_ODD(k_col_tma, 4, false);
+            else NBG_ODD(k_col_tma, 3, false);
+            break;
+        case JK_PWR: NBG_ODD(k_pwr, false, false); break;
+        case JK_PWR_SPLIT: NBG_ODD(k_pwr, true, false); break;
+        case JK_PWR_KEEP: NBG_ODD(k_pwr, false, true); break;
         case JK_REV:
-            if (smem <= COL4_MAX_SMEM) k_rev<4><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
-            else k_rev<3><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);
+            if (c4) NBG_ODD(k_rev, 4);
+            else NBG_ODD(k_rev, 3);
             break;
         case JK_UNPACK: k_unpack<<<grid, UNPACK_THREADS, smem, st>>>(prods, plans, jobs, njobs); break;
         case JK_CARRY: k_carry<<<grid, 256, 0, st>>>(prods, jobs, njobs); break;
@@ -1140,6 +1323,7 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
         }
         default: return cudaErrorInvalidValue;
     }
+#undef NBG_ODD
     return cudaGetLastError();
 }
 

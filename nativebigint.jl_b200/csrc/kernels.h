@@ -9,6 +9,8 @@ namespace nbg {
 // Uploads the prime constants and raises the kernels' dynamic shared-memory cap.
 cudaError_t kernels_init(double p1, double p2);
 int kernels_smem_optin();
+// reads and clears the count of bounded waits that gave up (current device)
+cudaError_t kernels_take_faults(unsigned int* n);
 // binaryVersion of the pass kernels as loaded on the current device
 cudaError_t kernels_binary_version(int* version);
 
@@ -21,8 +23,9 @@ inline JobSrc job_list(const Job* l) {
 }
 
 // One work-queue launch of `kind` (JobKind) over jobs 0..njobs-1 of `jobs`.
+// odd = false: no pass of the launch holds a radix-3/5/7 stage (a leaner kernel build).
 cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& jobs, int64_t njobs,
-                        size_t smem, int grid_cap, cudaStream_t st);
+                        size_t smem, int grid_cap, cudaStream_t st, bool odd = true);
 
 // Writes a batch's explicit job list from its compact description: out[g] for
 // every g < total, entry e covering [e.begin, e.begin + e.n).

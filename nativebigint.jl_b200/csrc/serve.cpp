@@ -279,9 +279,9 @@ bool nbg_server::launch_batch(std::unique_lock<std::mutex>& lk) {
         f.host_results.push_back({st_out + ro, q.r, 8 * (size_t)(q.m + q.n)});
         ro += up256(8 * (size_t)(q.m + q.n));
     }
-    bind_batch(f.bb, base);
+    bool ok = bind_batch(f.bb, base) == NBG_OK;
     stage_batch(f.bb, stage);
-    bool ok = cudaMemcpyAsync(base, stage, head, cudaMemcpyHostToDevice, f.st) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(base, stage, head, cudaMemcpyHostToDevice, f.st) == cudaSuccess;
     if (ok && host_in)
         ok = cudaMemcpyAsync(base + dev_in, stage + st_in, host_in, cudaMemcpyHostToDevice, f.st) == cudaSuccess;
     {

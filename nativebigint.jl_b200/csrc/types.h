@@ -75,7 +75,8 @@ struct DProd {
     int32_t plan;        // index into the device plan array
     int32_t npass;
     int32_t flags;       // PF_* bits
-    int32_t pad_;
+    int32_t tslot;       // TMA column passes: index of the product in its class's buffers (z = 2 * tslot + prime)
+    const void* tmap;    // TMA column passes: the class's tensor maps, 128 B each, [pass][operand]
     double* xa[2];       // per-prime transform buffers of operand a (and the result)
     double* xb[2];       // per-prime buffers of operand b (multi-pass products only)
     uint32_t* agg;       // per limb-tile carry aggregates (bit0 generate, bit1 propagate)
@@ -181,6 +182,8 @@ enum JobKind : int32_t {
     JK_CARRYFIX = 5, // carries through runs of all-ones limbs (one job per unpack tile)
     JK_PWR_SPLIT = 6,// JK_PWR with one job per prime (sub bit 1) for small batches
     JK_PWR_KEEP = 7, // JK_PWR for products with a kept operand spectrum (PF_BSAVE / PF_BSPEC)
+    JK_FWD_TMA = 8,  // JK_FWD with tiles staged by TMA (DProd.tmap; at least 16 columns per tile)
+    JK_REV_TMA = 9,  // JK_REV with tiles staged by TMA
 };
 
 constexpr int UNPACK_TL = 1024;  // output limbs per unpack tile

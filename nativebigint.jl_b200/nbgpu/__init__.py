@@ -40,7 +40,7 @@ EXPORTS = [
     "nbg_server_stats", "nbg_server_destroy",
     "nbg_powermod_batch", "nbg_powermod_batch_dev", "nbg_barrett_mu", "nbg_powmod_schedule",
     "nbg_mullo", "nbg_sqrlo", "nbg_matrix22_mul_dev", "nbg_mul2add_dev", "nbg_radix_combine",
-    "nbg_kernel_arch", "nbg_radix_powtab",
+    "nbg_kernel_arch", "nbg_radix_powtab", "nbg_device_faults",
 ]
 
 
@@ -115,6 +115,7 @@ def lib() -> ctypes.CDLL:
             "nbg_sqrlo": [vp, vp, i64, i64],
             "nbg_powermod_batch_dev": [vp, i64, i64, vp],
             "nbg_kernel_arch": [c.POINTER(i32)],
+            "nbg_device_faults": [c.POINTER(i64)],
             "nbg_radix_powtab": [vp, i64, c.POINTER(i64), i32, c.c_uint64, vp, i64, c.POINTER(i32)],
         }
         for name, args in sig.items():
@@ -335,8 +336,10 @@ class Batch:
         ops = (ctypes.c_double * n)()
         byt = (ctypes.c_double * n)()
         _check(lib().nbg_batch_stats(self._h, kinds, njobs, ops, byt, n))
-        names = {0: "k_fwd", 1: "k_pwr", 2: "k_rev", 3: "k_unpack", 4: "k_carry", 5: "k_carry_fix", 6: "k_pwr", 7: "k_pwr"}
-        return [dict(kind=names[kinds[i]], jobs=njobs[i], alg_ops=ops[i], alg_bytes=byt[i]) for i in range(n)]
+        names = {0: "k_fwd", 1: "k_pwr", 2: "k_rev", 3: "k_unpack", 4: "k_carry", 5: "k_carry_fix", 6: "k_pwr",
+                 7: "k_pwr", 8: "k_col_tma_fwd", 9: "k_col_tma_rev"}
+        return [dict(kind=names[kinds[i]], code=kinds[i], jobs=njobs[i], alg_ops=ops[i], alg_bytes=byt[i])
+                for i in range(n)]
 
     def profile(self, stream=None) -> list[float]:
         n = self.launches
@@ -568,6 +571,13 @@ def load_tuning(path: str) -> None:
 def trim_plans() -> None:
     """Frees cached plans' device tables (no Batch may be alive)."""
     _check(lib().nbg_trim_plans())
+
+
+def device_faults() -> int:
+    """Bounded kernel waits that gave up since the last call (0 when healthy); clears the count."""
+    n = ctypes.c_int64()
+    _check(lib().nbg_device_faults(ctypes.byref(n)))
+    return n.value
 
 
 def version() -> str:

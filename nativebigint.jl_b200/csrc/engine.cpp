@@ -373,8 +373,10 @@ int plan_structure(int64_t N, int for_sqr, const Tuning& tun, DPlan& d) {
     for (int64_t v : okm) okm_hit |= (m == v);
     if (!okm_hit || !(m == 1 || k >= 2) || k > std::min(TWOADIC[0], TWOADIC[1]))
         return fail(NBG_EINVAL, "inadmissible transform length %lld", (long long)N);
-    // device indices are 32-bit: 2^31 points is a 16 GB transform buffer
-    if (N >= (int64_t(1) << 31)) return fail(NBG_ENOMEM, "transform length %lld too large for one GPU", (long long)N);
+    // Tile coordinates and in-tile offsets are 32-bit, global offsets 64-bit:
+    // lengths up to 2^32 points (a square there needs about 140 GB of HBM).
+    if (N > (int64_t(1) << 32))
+        return fail(NBG_ENOMEM, "transform length %lld is beyond one GPU (at most 2^32 points)", (long long)N);
 
     memset(&d, 0, sizeof d);
     d.N = N;

@@ -113,7 +113,7 @@ template <int M, bool FWD, bool PAD>
 __device__ NBG_ROUND void round_gen(const Tiles& T, const DStage& st) {
     const int C = 1 << T.lc;
     const int Lloc = (int)(st.L / T.Qb), Qloc = (int)(st.Q / T.Qb);
-    const int Q = (int)st.Q;
+    const int64_t Q = st.Q;  // twiddle rows are Q apart (up to N/3)
     const int per = (T.G / M) << T.lc;
     const int total = per * T.ntiles;
     // row / Qloc = (row >> e) / odd, odd by multiply-high (exact for rows < 2^32 / odd)
@@ -170,7 +170,7 @@ __device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStag
     const int C = 1 << T.lc;
     const int Lloc = (int)(A.L / T.Qb);
     const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
-    const int QA = (int)A.Q, QB = (int)B.Q;
+    const int64_t QA = A.Q, QB = B.Q;  // twiddle rows (up to N/4 apart)
     const int per = (T.G >> 4) << T.lc;
     const int total = per * T.ntiles;
     const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];  // the same 4th root for every radix-4 stage
@@ -194,7 +194,7 @@ __device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStag
         const int jB = j2 * T.Qb + T.j0 + c;
         const double* twB = (p1 ? twB1 : twB0) + jB;
         const double* twA = (p1 ? twA1 : twA0) + jB;  // A's column for t2 is jB + t2*q16*Qb
-        const int stepA = q16 * T.Qb;
+        const int64_t stepA = (int64_t)q16 * T.Qb;
         if (FWD) {
 #pragma unroll
             for (int t2 = 0; t2 < 4; t2++) {
@@ -291,7 +291,7 @@ __device__ __forceinline__ void pw4(double* a, const double* b, Fp F) {
 }
 
 template <bool FWD>
-__device__ __forceinline__ void r16_body(double* v, const double* twA, int stepA, int QA, const double* wB,
+__device__ __forceinline__ void r16_body(double* v, const double* twA, int64_t stepA, int64_t QA, const double* wB,
                                          double wi, Fp F) {
     if (FWD) {
 #pragma unroll
@@ -322,7 +322,7 @@ __device__ NBG_ROUND void fused_r16(const FuseTiles& T, const DStage& A, const D
     const int C = 1 << T.lc;
     const int Lloc = (int)(A.L / T.Qb);
     const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
-    const int QA = (int)A.Q, QB = (int)B.Q;
+    const int64_t QA = A.Q, QB = B.Q;
     const int per = (T.G >> 4) << T.lc;
     const int total = T.pfix >= 0 ? per : 2 * per;
     const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
@@ -342,7 +342,7 @@ __device__ NBG_ROUND void fused_r16(const FuseTiles& T, const DStage& A, const D
         const int jB = j2 * T.Qb + T.j0 + c;
         const double* twB = (p1 ? twB1 : twB0) + jB;
         const double* twA = (p1 ? twA1 : twA0) + jB;
-        const int stepA = q16 * T.Qb;
+        const int64_t stepA = (int64_t)q16 * T.Qb;
         const double wB[4] = {0.0, __ldg(twB), __ldg(twB + QB), __ldg(twB + 2 * QB)};
         double va[16];
         if (!T.sq && !T.bspec) {
@@ -465,13 +465,11 @@ __device__ void run_pass(const Tiles& T, const DPlan& pl, const DPass& ps) {
 }
 
 // Tile geometry: tile t of pass ps -> global index of its (row 0, column 0) and its first column.
-__device__ __forceinline__ void tile_geo(const DPlan& pl, const DPass& ps, int64_t t, int& base, int& j0) {
-    const int per = (int)(ps.Qb / ps.C);
-    const int tt = (int)t;
-    const int blk = tt / per;
-    const int jc = tt - blk * per;
-    j0 = jc * ps.C;
-    base = blk * (int)pl.st[ps.sa].L + j0;
+__device__ __forceinline__ void tile_geo(const DPlan& pl, const DPass& ps, int64_t t, int64_t& base, int& j0) {
+    const int64_t per = ps.Qb / ps.C;
+    const int64_t blk = t / per;
+    j0 = (int)((t - blk * per) * ps.C);
+    base = blk * pl.st[ps.sa].L + j0;
 }
 
 // Asynchronous global -> shared copies (cp.async, 8 bytes each): a thread
@@ -485,19 +483,21 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // x[base + c + k*Qb] -> tile row k, column c (padded).  Issues only; the
 // caller waits with cp_async_wait_all() and a barrier.
-__device__ __forceinline__ void load_tile_async(double* s, const double* __restrict__ x, const DPass& ps, int base) {
+__device__ __forceinline__ void load_tile_async(double* s, const double* __restrict__ x, const DPass& ps,
+                                                int64_t base) {
     const int lc = __ffs(ps.C) - 1;
     const int n = ps.G << lc;
-    const int Qb = (int)ps.Qb;
+    const int64_t Qb = ps.Qb;
+    x += base;
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
         const int k = e >> lc, c = e & (ps.C - 1);
-        cp_async8(s + sp(e), x + base + c + k * Qb);
+        cp_async8(s + sp(e), x + c + k * Qb);
     }
 }
-__device__ __forceinline__ void store_tile(const double* s, double* __restrict__ x, const DPass& ps, int base) {
+__device__ __forceinline__ void store_tile(const double* s, double* __restrict__ x, const DPass& ps, int64_t base) {
     const int lc = __ffs(ps.C) - 1;
     const int n = ps.G << lc;
-    const int Qb = (int)ps.Qb;
+    const int64_t Qb = ps.Qb;
     const int nt = blockDim.x;
     int e = threadIdx.x;
     // batches of 4 shared loads ahead of their global stores
@@ -584,7 +584,8 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restr
         const DPlan& pl = plans[P.plan];
         const int opb = (jb.sub >> 1) & 1, pass = (jb.sub >> 8) & 0xff;
         const DPass& ps = pl.pass[pass];
-        int base, j0;
+        int64_t base;
+        int j0;
         tile_geo(pl, ps, jb.tile, base, j0);
         const int stride = tile_stride_doubles(ps.G * ps.C);
         double* s0 = smem;
@@ -622,7 +623,8 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
         const DPlan& pl = plans[P.plan];
         const int pass = P.npass - 1;
         const DPass& ps = pl.pass[pass];
-        int base, j0;
+        int64_t base;
+        int j0;
         tile_geo(pl, ps, jb.tile, base, j0);
         const int stride = tile_stride_doubles(ps.G * ps.C);
         const int sq = P.sqr;
@@ -735,7 +737,8 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_rev(const DProd* __restr
         const DPlan& pl = plans[P.plan];
         const int pass = (jb.sub >> 8) & 0xff;
         const DPass& ps = pl.pass[pass];
-        int base, j0;
+        int64_t base;
+        int j0;
         tile_geo(pl, ps, jb.tile, base, j0);
         const int stride = tile_stride_doubles(ps.G * ps.C);
         __syncthreads();

@@ -53,7 +53,9 @@ def test_square_beyond_2_31_points(gpu_lib):
     bch, N = gpu_lib.ntt_params(64 * n, 64 * n)
     assert N > 2**31
     gen = torch.Generator(device="cuda").manual_seed(62)
-    da = torch.randint(-2**63, 2**63 - 1, (n,), dtype=torch.int64, device="cuda", generator=gen)
+    # uniform 64-bit limbs: 62 random bits shifted up (wrapping) plus 2 more
+    da = torch.randint(0, 2**62, (n,), dtype=torch.int64, device="cuda", generator=gen) * 4
+    da += torch.randint(0, 4, (n,), dtype=torch.int64, device="cuda", generator=gen)
     da[-1] = 12345  # top limb nonzero
     da = da.view(torch.uint64)
     r = torch.empty(2 * n, dtype=torch.uint64, device="cuda")

@@ -113,7 +113,8 @@ template <int M, bool FWD, bool PAD>
 __device__ NBG_ROUND void round_gen(const Tiles& T, const DStage& st) {
     const int C = 1 << T.lc;
     const int Lloc = (int)(st.L / T.Qb), Qloc = (int)(st.Q / T.Qb);
-    const int64_t Q = st.Q;  // twiddle rows are Q apart (up to N/3)
+    // twiddle offsets stay below N <= 2^32: 32-bit unsigned arithmetic
+    const uint32_t Q = (uint32_t)st.Q;
     const int per = (T.G / M) << T.lc;
     const int total = per * T.ntiles;
     // row / Qloc = (row >> e) / odd, odd by multiply-high (exact for rows < 2^32 / odd)
@@ -170,7 +171,8 @@ __device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStag
     const int C = 1 << T.lc;
     const int Lloc = (int)(A.L / T.Qb);
     const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
-    const int64_t QA = A.Q, QB = B.Q;  // twiddle rows (up to N/4 apart)
+    // twiddle offsets (t2 * stepA + 2 * QA < L_A <= N <= 2^32): 32-bit unsigned
+    const uint32_t QA = (uint32_t)A.Q, QB = (uint32_t)B.Q;
     const int per = (T.G >> 4) << T.lc;
     const int total = per * T.ntiles;
     const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];  // the same 4th root for every radix-4 stage
@@ -194,7 +196,7 @@ __device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStag
         const int jB = j2 * T.Qb + T.j0 + c;
         const double* twB = (p1 ? twB1 : twB0) + jB;
         const double* twA = (p1 ? twA1 : twA0) + jB;  // A's column for t2 is jB + t2*q16*Qb
-        const int64_t stepA = (int64_t)q16 * T.Qb;
+        const uint32_t stepA = (uint32_t)q16 * (uint32_t)T.Qb;
         if (FWD) {
 #pragma unroll
             for (int t2 = 0; t2 < 4; t2++) {
@@ -291,7 +293,7 @@ __device__ __forceinline__ void pw4(double* a, const double* b, Fp F) {
 }
 
 template <bool FWD>
-__device__ __forceinline__ void r16_body(double* v, const double* twA, int64_t stepA, int64_t QA, const double* wB,
+__device__ __forceinline__ void r16_body(double* v, const double* twA, uint32_t stepA, uint32_t QA, const double* wB,
                                          double wi, Fp F) {
     if (FWD) {
 #pragma unroll
@@ -322,7 +324,7 @@ __device__ NBG_ROUND void fused_r16(const FuseTiles& T, const DStage& A, const D
     const int C = 1 << T.lc;
     const int Lloc = (int)(A.L / T.Qb);
     const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
-    const int64_t QA = A.Q, QB = B.Q;
+    const uint32_t QA = (uint32_t)A.Q, QB = (uint32_t)B.Q;
     const int per = (T.G >> 4) << T.lc;
     const int total = T.pfix >= 0 ? per : 2 * per;
     const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
@@ -342,7 +344,7 @@ __device__ NBG_ROUND void fused_r16(const FuseTiles& T, const DStage& A, const D
         const int jB = j2 * T.Qb + T.j0 + c;
         const double* twB = (p1 ? twB1 : twB0) + jB;
         const double* twA = (p1 ? twA1 : twA0) + jB;
-        const int64_t stepA = (int64_t)q16 * T.Qb;
+        const uint32_t stepA = (uint32_t)q16 * (uint32_t)T.Qb;
         const double wB[4] = {0.0, __ldg(twB), __ldg(twB + QB), __ldg(twB + 2 * QB)};
         double va[16];
         if (!T.sq && !T.bspec) {

@@ -897,12 +897,11 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __r
 // five) coefficients overlapping bits [64w, 64w+64).  This equals the
 // reference's S1 + p1*S2 fold (:793-795, :923) as an integer, so the limbs are
 // identical.
-__device__ __forceinline__ void garner(const double* __restrict__ x1, const double* __restrict__ x2, int64_t idx,
-                                       const DPlan& pl, uint64_t& lo, uint64_t& hi) {
+__device__ __forceinline__ void garner_xy(double x1v, double x2v, const DPlan& pl, uint64_t& lo, uint64_t& hi) {
     const Fp F1 = fpctx(0), F2 = fpctx(1);
-    double v1 = fp_mulmod4(__ldg(x1 + idx), pl.ninv[0], pl.ninvp[0], F1);
+    double v1 = fp_mulmod4(x1v, pl.ninv[0], pl.ninvp[0], F1);
     v1 = v1 < 0.0 ? dadd(v1, F1.p) : v1;
-    double v2 = fp_mulmod4(__ldg(x2 + idx), pl.ninv[1], pl.ninvp[1], F2);
+    double v2 = fp_mulmod4(x2v, pl.ninv[1], pl.ninvp[1], F2);
     double u = fp_mulmod4(dsub(v2, fp_reduce(v1, F2)), c_garner[0], c_garner[1], F2);
     u = u < 0.0 ? dadd(u, F2.p) : u;
     // canonical values are < 2^50: adding 1.5*2^52 leaves them in the low 51
@@ -915,6 +914,11 @@ __device__ __forceinline__ void garner(const double* __restrict__ x1, const doub
     uint64_t phi = __umul64hi(uu, P1_U);
     lo = plo + c1;
     hi = phi + (lo < plo ? 1ULL : 0ULL);
+}
+
+__device__ __forceinline__ void garner(const double* __restrict__ x1, const double* __restrict__ x2, int64_t idx,
+                                       const DPlan& pl, uint64_t& lo, uint64_t& hi) {
+    garner_xy(__ldg(x1 + idx), __ldg(x2 + idx), pl, lo, hi);
 }
 
 constexpr int UNPACK_THREADS = 256;
@@ -989,12 +993,29 @@ __global__ void __launch_bounds__(UNPACK_THREADS, 4) k_unpack(const DProd* __res
         if (ihi > P.nconv - 1) ihi = P.nconv - 1;
         const int64_t ncoef = ihi >= ilo ? ihi - ilo + 1 : 0;
         __syncthreads();
-        for (int64_t k = threadIdx.x; k < ncoef; k += blockDim.x) {
-            const int64_t i = ilo + k;
-            const int64_t idx = i == 0 ? 0 : N - i;
-            uint64_t lo, hi;
-            garner(P.xa[0], P.xa[1], idx, pl, lo, hi);
-            ucs[k] = make_ulonglong2(lo, hi);
+        // Garner, four coefficients per thread at a time: their eight loads are
+        // in flight together before the arithmetic
+        const double* __restrict__ x1 = P.xa[0];
+        const double* __restrict__ x2 = P.xa[1];
+        for (int64_t k0 = threadIdx.x; k0 < ncoef; k0 += 4 * (int64_t)blockDim.x) {
+            double a1[4], a2[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int64_t k = k0 + q * (int64_t)blockDim.x;
+                const int64_t i = ilo + k;
+                const int64_t idx = k < ncoef ? (i == 0 ? 0 : N - i) : 0;
+                a1[q] = __ldg(x1 + idx);
+                a2[q] = __ldg(x2 + idx);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int64_t k = k0 + q * (int64_t)blockDim.x;
+                if (k < ncoef) {
+                    uint64_t lo, hi;
+                    garner_xy(a1[q], a2[q], pl, lo, hi);
+                    ucs[k] = make_ulonglong2(lo, hi);
+                }
+            }
         }
         __syncthreads();
         const int t = threadIdx.x;
@@ -1303,12 +1324,14 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
             if (c4) NBG_ODD(k_fwd, 4);
             else NBG_ODD(k_fwd, 3);
             break;
+        // passes with radix-3/5/7 rounds take the 80-register build whatever
+        // their tile size (the 64-register one spills there)
         case JK_FWD_TMA:
-            if (c4t) NBG_ODD(k_col_tma, 4, true);
+            if (c4t && !odd) NBG_ODD(k_col_tma, 4, true);
             else NBG_ODD(k_col_tma, 3, true);
             break;
         case JK_REV_TMA:
-            if (c4t) NBG_ODD(k_col_tma, 4, false);
+            if (c4t && !odd) NBG_ODD(k_col_tma, 4, false);
             else NBG_ODD(k_col_tma, 3, false);
             break;
         case JK_PWR: NBG_ODD(k_pwr, false, false); break;

@@ -229,6 +229,100 @@ __device__ NBG_ROUND void round_r16(const Tiles& T, const DStage& A, const DStag
     }
 }
 
+// ---------------------------------------------------------------------------
+// Radix-16 round on a dense tile (the TMA column passes), with the distance
+// between a unit's 16 points, 2^LS elements, known at compile time and the
+// prime's constants taken from constant memory by a compile-time index: every
+// shared-memory access is one base register plus an immediate offset, and no
+// register holds or selects the field constants.  Same butterflies, same
+// inputs, same order as round_r16.
+
+// One radix-4 butterfly of the reference on four named values (butterfly<4>).
+template <bool FWD>
+__device__ __forceinline__ void bf4(double& a, double& b, double& c, double& d, double w1, double w2, double w3,
+                                    double wi, const Fp F) {
+    if (FWD) dft4(a, b, c, d, wi, F);
+    a = fp_reduce(a, F);
+    b = fp_mulmod(b, w1, F);
+    c = fp_mulmod(c, w2, F);
+    d = fp_mulmod(d, w3, F);
+    if (!FWD) dft4(a, b, c, d, wi, F);
+}
+
+template <bool FWD, int LS, int PR>
+__device__ __forceinline__ void r16_unit_dense(double* __restrict__ s, const double* __restrict__ twA,
+                                               const double* __restrict__ twB, uint32_t stepA, uint32_t QA,
+                                               uint32_t QB, double wi) {
+    const Fp F = c_fp[PR];
+    double v[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = s[k << LS];
+    if (FWD) {
+#pragma unroll
+        for (int t2 = 0; t2 < 4; t2++) {
+            const double* ta = twA + t2 * stepA;
+            bf4<true>(v[t2], v[4 + t2], v[8 + t2], v[12 + t2], __ldg(ta), __ldg(ta + QA), __ldg(ta + 2 * QA), wi, F);
+        }
+        const double b1 = __ldg(twB), b2 = __ldg(twB + QB), b3 = __ldg(twB + 2 * QB);
+#pragma unroll
+        for (int t1 = 0; t1 < 4; t1++)
+            bf4<true>(v[4 * t1], v[4 * t1 + 1], v[4 * t1 + 2], v[4 * t1 + 3], b1, b2, b3, wi, F);
+    } else {
+        const double b1 = __ldg(twB), b2 = __ldg(twB + QB), b3 = __ldg(twB + 2 * QB);
+#pragma unroll
+        for (int t1 = 0; t1 < 4; t1++)
+            bf4<false>(v[4 * t1], v[4 * t1 + 1], v[4 * t1 + 2], v[4 * t1 + 3], b1, b2, b3, wi, F);
+#pragma unroll
+        for (int t2 = 0; t2 < 4; t2++) {
+            const double* ta = twA + t2 * stepA;
+            bf4<false>(v[t2], v[4 + t2], v[8 + t2], v[12 + t2], __ldg(ta), __ldg(ta + QA), __ldg(ta + 2 * QA), wi, F);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 16; k++) s[k << LS] = v[k];
+}
+
+// Tiles: prime 0 at T.s, prime 1 at T.s + T.stride (dense, row length C = 2^lc).
+template <bool FWD, int LS>
+__device__ NBG_ROUND void round_r16_dense(const Tiles& T, const DStage& A, const DStage& B) {
+    const int lc = T.lc;
+    const int C = 1 << lc;
+    const int Lloc = (int)(A.L / T.Qb);
+    const int q16 = Lloc >> 4, lq = __ffs(q16) - 1;
+    const int per = (T.G >> 4) << lc;
+    const uint32_t QA = (uint32_t)A.Q, QB = (uint32_t)B.Q;
+    const uint32_t stepA = (uint32_t)q16 * (uint32_t)T.Qb;
+    const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
+    const double *twA0 = A.tw[0], *twA1 = A.tw[1], *twB0 = B.tw[0], *twB1 = B.tw[1];
+    for (int u = threadIdx.x; u < 2 * per; u += blockDim.x) {
+        const bool p1 = u >= per;
+        const int uu = p1 ? u - per : u;
+        const int c = uu & (C - 1);
+        const int r = uu >> lc;
+        const int b = r >> lq, j2 = r & (q16 - 1);
+        const int base = ((b * Lloc + j2) << lc) + c;
+        const uint32_t jB = (uint32_t)j2 * (uint32_t)T.Qb + (uint32_t)(T.j0 + c);
+        if (p1) r16_unit_dense<FWD, LS, 1>(T.s + T.stride + base, twA1 + jB, twB1 + jB, stepA, QA, QB, wi1);
+        else r16_unit_dense<FWD, LS, 0>(T.s + base, twA0 + jB, twB0 + jB, stepA, QA, QB, wi0);
+    }
+}
+
+template <bool FWD>
+__device__ __forceinline__ void round_r16_dense_any(const Tiles& T, const DStage& A, const DStage& B) {
+    const int ls = (__ffs((int)(A.L / T.Qb)) - 1 - 4) + T.lc;  // log2(q16 * C)
+    switch (ls) {
+        case 4: round_r16_dense<FWD, 4>(T, A, B); break;
+        case 5: round_r16_dense<FWD, 5>(T, A, B); break;
+        case 6: round_r16_dense<FWD, 6>(T, A, B); break;
+        case 7: round_r16_dense<FWD, 7>(T, A, B); break;
+        case 8: round_r16_dense<FWD, 8>(T, A, B); break;
+        case 9: round_r16_dense<FWD, 9>(T, A, B); break;
+        case 10: round_r16_dense<FWD, 10>(T, A, B); break;
+        case 11: round_r16_dense<FWD, 11>(T, A, B); break;
+        default: round_r16<FWD, false>(T, A, B); break;
+    }
+}
+
 // Radix-8 round: the span-8 radix-4 stage A (Q = 2) and the radix-2 stage, on
 // 8 consecutive points (contiguous passes only: C = 1, Qb = 1, j0 = 0).
 template <bool FWD>
@@ -439,7 +533,10 @@ __device__ void run_round(const Tiles& T, const DPlan& pl, int kind, int s0) {
     __syncthreads();
     const DStage& st = pl.st[s0];
     switch (kind) {
-        case RK_R16: round_r16<FWD, PAD>(T, st, pl.st[s0 + 1]); break;
+        case RK_R16:
+            if (PAD) round_r16<FWD, PAD>(T, st, pl.st[s0 + 1]);
+            else round_r16_dense_any<FWD>(T, st, pl.st[s0 + 1]);
+            break;
         case RK_R4: round_gen<4, FWD, PAD>(T, st); break;
         case RK_R8:
             if (PAD) round_r8<FWD>(T, st);

@@ -294,15 +294,18 @@ __device__ NBG_ROUND void round_r16_dense(const Tiles& T, const DStage& A, const
     const uint32_t stepA = (uint32_t)q16 * (uint32_t)T.Qb;
     const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
     const double *twA0 = A.tw[0], *twA1 = A.tw[1], *twB0 = B.tw[0], *twB1 = B.tw[1];
-    for (int u = threadIdx.x; u < 2 * per; u += blockDim.x) {
-        const bool p1 = u >= per;
-        const int uu = p1 ? u - per : u;
+    // pfix >= 0: the tiles hold that prime alone (at T.s)
+    const int total = T.pfix >= 0 ? per : 2 * per;
+    double* const s1 = T.pfix >= 0 ? T.s : T.s + T.stride;
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : u >= per;
+        const int uu = (T.pfix < 0 && p1) ? u - per : u;
         const int c = uu & (C - 1);
         const int r = uu >> lc;
         const int b = r >> lq, j2 = r & (q16 - 1);
         const int base = ((b * Lloc + j2) << lc) + c;
         const uint32_t jB = (uint32_t)j2 * (uint32_t)T.Qb + (uint32_t)(T.j0 + c);
-        if (p1) r16_unit_dense<FWD, LS, 1>(T.s + T.stride + base, twA1 + jB, twB1 + jB, stepA, QA, QB, wi1);
+        if (p1) r16_unit_dense<FWD, LS, 1>(s1 + base, twA1 + jB, twB1 + jB, stepA, QA, QB, wi1);
         else r16_unit_dense<FWD, LS, 0>(T.s + base, twA0 + jB, twB0 + jB, stepA, QA, QB, wi0);
     }
 }
@@ -931,22 +934,60 @@ __device__ __forceinline__ void tile_box(const DPass& ps, int64_t t, int& x, int
     y = (int)(blk * ps.G);
 }
 
-// One column pass (forward or reverse) of one tile of one operand, both primes,
-// staged by TMA.  Dynamic shared memory: [mbarrier | 120 B | tiles].
+// One column pass (forward or reverse) of a run of tiles, staged by TMA and
+// pipelined by prime.  A CTA walks its jobs as half-jobs h = (job, prime) with
+// one shared-memory buffer per prime: at the start of half-job h, thread 0
+// waits until the store of half-job h - 1 has read its buffer and issues the
+// load of half-job h + 1 into it, so that load runs while half-job h is
+// transformed.  Dynamic shared memory: [2 mbarriers | 112 B | buffer 0 |
+// buffer 1], each buffer one G x C tile.  Pass 0 of a forward transform packs
+// limbs instead of loading: the pack is written into both buffers at the
+// job's first half (both tiles hold the same chunks).
 template <int MINB, bool FWD, bool ODD>
 __global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __restrict__ prods,
                                                              const DPlan* __restrict__ plans,
                                                              const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ __align__(128) double dsm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm);
-    double* smem = dsm + 16;  // tiles start 128 bytes in
-    if (threadIdx.x == 0) tma::bar_init(bar);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm);  // bar[0], bar[1]
+    double* smem = dsm + 16;                           // buffers start 128 bytes in
+    if (threadIdx.x == 0) {
+        tma::bar_init(bar);
+        tma::bar_init(bar + 1);
+    }
     __syncthreads();
-    uint32_t phase = 0;
+    uint32_t phase[2] = {0, 0};
     const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
-    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
-    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
-        const Job jb = jobs[ji];
+    const int64_t j0 = (int64_t)blockIdx.x * run;
+    const int64_t jend = min(njobs, j0 + run);
+    if (j0 >= jend) return;
+    const int64_t nhalf = 2 * (jend - j0);
+    // every job of a launch has the same tile size
+    int cnt;
+    {
+        const Job jb = jobs[j0];
+        const DPass& ps = plans[prods[jb.prod].plan].pass[(jb.sub >> 8) & 0xff];
+        cnt = ps.G * ps.C;
+    }
+    // issues the load of half-job h (thread 0), unless its job packs limbs
+    auto issue = [&](int64_t h) {
+        const Job jb = jobs[j0 + (h >> 1)];
+        const int f = (int)(h & 1);
+        const DProd& P = prods[jb.prod];
+        const int pass = (jb.sub >> 8) & 0xff;
+        if (FWD && pass == 0 && !(P.flags & PF_PRELOADED)) return;
+        const int opb = FWD ? (jb.sub >> 1) & 1 : 0;
+        const DPass& ps = plans[P.plan].pass[pass];
+        int x, y;
+        tile_box(ps, jb.tile, x, y);
+        const void* map = static_cast<const char*>(P.tmap) + 128 * (2 * pass + opb);
+        tma::fence_map(map);
+        tma::bar_expect(bar + f, (uint32_t)(cnt * sizeof(double)));
+        tma::load3(smem + f * cnt, map, x, y, 2 * P.tslot + f, bar + f);
+    };
+    if (threadIdx.x == 0) issue(0);
+    for (int64_t h = 0; h < nhalf; h++) {
+        const Job jb = jobs[j0 + (h >> 1)];
+        const int f = (int)(h & 1);
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int opb = FWD ? (jb.sub >> 1) & 1 : 0;
@@ -954,35 +995,34 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __r
         const DPass& ps = pl.pass[pass];
         int x, y;
         tile_box(ps, jb.tile, x, y);
-        const int z = 2 * P.tslot;
         const void* map = static_cast<const char*>(P.tmap) + 128 * (2 * pass + opb);
-        const int cnt = ps.G * ps.C;
         const bool pack = FWD && pass == 0 && !(P.flags & PF_PRELOADED);
-        __syncthreads();  // every thread is done with the previous tile
+        double* buf = smem + f * cnt;
+        __syncthreads();  // every thread is done with half-job h - 1
         if (threadIdx.x == 0) {
-            tma::stores_read();  // the previous tile's store has read shared memory
-            if (!pack) {
-                tma::fence_map(map);
-                tma::bar_expect(bar, (uint32_t)(2 * cnt * sizeof(double)));
-                tma::load3(smem, map, x, y, z, bar);
-            }
+            tma::stores_read();  // the store of half-job h - 1 has read its buffer
+            if (h + 1 < nhalf) issue(h + 1);
         }
         if (pack) {
-            __syncthreads();
-            const int64_t base = (int64_t)(y / ps.G) * pl.st[ps.sa].L + x;
-            if (opb) pack_tile2<false>(smem, smem + cnt, P.b, P.n, P.bch, P.ncb, ps, base);
-            else pack_tile2<false>(smem, smem + cnt, P.a, P.m, P.bch, P.nca, ps, base);
+            if (f == 0) {  // both primes' tiles hold the same chunks
+                __syncthreads();
+                const int64_t base = (int64_t)(y / ps.G) * pl.st[ps.sa].L + x;
+                if (opb) pack_tile2<false>(smem, smem + cnt, P.b, P.n, P.bch, P.ncb, ps, base);
+                else pack_tile2<false>(smem, smem + cnt, P.a, P.m, P.bch, P.nca, ps, base);
+            }
         } else {
-            if (!tma::bar_wait(bar, phase)) {  // gave up: leave after the stores issued so far
+            if (!tma::bar_wait(bar + f, phase[f])) {  // gave up: leave after the stores issued so far
                 if (threadIdx.x == 0) tma::stores_done();
                 return;
             }
-            phase ^= 1u;
+            phase[f] ^= 1u;
         }
-        run_pass<FWD, false, ODD>(make_tiles(smem, cnt, 2, 0, ps, x), pl, ps);
+        Tiles T = make_tiles(buf, cnt, 1, 30, ps, x);
+        T.pfix = f;
+        run_pass<FWD, false, ODD>(T, pl, ps);
         tma::fence_async();
         __syncthreads();
-        if (threadIdx.x == 0) tma::store3(map, x, y, z, smem);
+        if (threadIdx.x == 0) tma::store3(map, x, y, 2 * P.tslot + f, buf);
     }
     if (threadIdx.x == 0) tma::stores_done();
 }
@@ -1068,6 +1108,15 @@ __device__ __forceinline__ void range_limbs(const ulonglong2* __restrict__ cs, i
     s1 = W1;
 }
 
+// floor(x / b) for 0 <= x < 2^50 and 1 <= b <= 52 without a 64-bit integer
+// division: the double quotient is off by at most one, fixed by an exact check.
+__device__ __forceinline__ int64_t div_b(int64_t x, int b, double rb) {
+    int64_t q = (int64_t)__dmul_rn((double)x, rb);
+    if (q * b > x) q--;
+    else if ((q + 1) * b <= x) q++;
+    return q;
+}
+
 __global__ void __launch_bounds__(UNPACK_THREADS, 4) k_unpack(const DProd* __restrict__ prods,
                                                               const DPlan* __restrict__ plans,
                                                               const Job* __restrict__ jobs, int64_t njobs) {
@@ -1085,8 +1134,9 @@ __global__ void __launch_bounds__(UNPACK_THREADS, 4) k_unpack(const DProd* __res
         // coefficients that start in bits [64 (w0 - 4), 64 w1): the tile's own and
         // those of the 4-limb range below it, whose spill reaches limb w0
         const int64_t wlo = w0 >= 4 ? w0 - 4 : 0;
-        const int64_t ilo = (64 * wlo + b - 1) / b;
-        int64_t ihi = (64 * w1 - 1) / b;
+        const double rb = 1.0 / (double)b;
+        const int64_t ilo = div_b(64 * wlo + b - 1, b, rb);
+        int64_t ihi = div_b(64 * w1 - 1, b, rb);
         if (ihi > P.nconv - 1) ihi = P.nconv - 1;
         const int64_t ncoef = ihi >= ilo ? ihi - ilo + 1 : 0;
         __syncthreads();
@@ -1119,8 +1169,8 @@ __global__ void __launch_bounds__(UNPACK_THREADS, 4) k_unpack(const DProd* __res
         const int64_t wt = w0 + 4 * (int64_t)t;
         uint64_t own[4], s0, s1;
         {
-            const int64_t i0 = (64 * wt + b - 1) / b;
-            const int64_t i1 = min((64 * (wt + 4) - 1) / b, ihi);
+            const int64_t i0 = div_b(64 * wt + b - 1, b, rb);
+            const int64_t i1 = min(div_b(64 * (wt + 4) - 1, b, rb), ihi);
             range_limbs<true>(ucs, ilo, i0, i1, (uint32_t)(b * i0 - 64 * wt), (uint32_t)b, own, s0, s1);
         }
         spill[t + 1][0] = s0;
@@ -1129,7 +1179,7 @@ __global__ void __launch_bounds__(UNPACK_THREADS, 4) k_unpack(const DProd* __res
             uint64_t p0 = 0, p1 = 0;
             if (w0 > 0) {  // the spill of the range [w0 - 4, w0) into limbs w0, w0 + 1
                 const int64_t i0 = ilo;
-                const int64_t i1 = min((64 * w0 - 1) / b, ihi);
+                const int64_t i1 = min(div_b(64 * w0 - 1, b, rb), ihi);
                 range_limbs<false>(ucs, ilo, i0, i1, (uint32_t)(b * i0 - 64 * wlo), (uint32_t)b, nullptr, p0, p1);
             }
             spill[0][0] = p0;

@@ -911,7 +911,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         for (int p = 0; p < Pn - 1; p++) {
             const DPass& ps = pl.pass[p];
             const bool tp = (tmask >> p) & 1u;
-            const size_t smem = tp ? 128 + sizeof(double) * 2 * (size_t)(ps.G * ps.C)
+            const size_t smem = tp ? 128 + sizeof(double) * (size_t)(ps.G * ps.C)
                                    : sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
             const double jobs = (double)ps.ntiles * nop * nc;
@@ -941,7 +941,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         for (int p = Pn - 2; p >= 0; p--) {
             const DPass& ps = pl.pass[p];
             const bool tp = (tmask >> p) & 1u;
-            const size_t smem = tp ? 128 + sizeof(double) * 2 * (size_t)(ps.G * ps.C)
+            const size_t smem = tp ? 128 + sizeof(double) * (size_t)(ps.G * ps.C)
                                    : sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
             const double jobs = (double)ps.ntiles * nc;

@@ -38,7 +38,6 @@
 #endif
 // Column passes with tile sets up to this size run the 4-CTA/SM build.
 constexpr size_t COL4_MAX_SMEM = 32 * 1024;
-constexpr size_t COL4_MAX_SMEM_TMA = 32 * 1024 + 128;  // the TMA tiles plus their mbarrier line
 // Rounds are inlined into the kernels; out-of-line rounds (NBG_ROUND_NOINLINE)
 // measured 40% slower in k_pwr.
 #ifdef NBG_ROUND_NOINLINE
@@ -249,14 +248,22 @@ __device__ __forceinline__ void bf4(double& a, double& b, double& c, double& d, 
     if (!FWD) dft4(a, b, c, d, wi, F);
 }
 
-template <bool FWD, int LS, int PR>
+// Offset of a unit's point k from its point 0: 2^LS elements apart, or on a
+// padded tile (one double in 16) with single columns, where the unit's first
+// point sits below a multiple of 2^LS + ... so the padding adds (k 2^LS) / 16.
+template <int LS, bool PADL>
+__device__ __forceinline__ constexpr int r16_off(int k) {
+    return PADL ? (k << LS) + ((k << LS) >> 4) : (k << LS);
+}
+
+template <bool FWD, int LS, int PR, bool PADL = false>
 __device__ __forceinline__ void r16_unit_dense(double* __restrict__ s, const double* __restrict__ twA,
                                                const double* __restrict__ twB, uint32_t stepA, uint32_t QA,
                                                uint32_t QB, double wi) {
     const Fp F = c_fp[PR];
     double v[16];
 #pragma unroll
-    for (int k = 0; k < 16; k++) v[k] = s[k << LS];
+    for (int k = 0; k < 16; k++) v[k] = s[r16_off<LS, PADL>(k)];
     if (FWD) {
 #pragma unroll
         for (int t2 = 0; t2 < 4; t2++) {
@@ -279,7 +286,47 @@ __device__ __forceinline__ void r16_unit_dense(double* __restrict__ s, const dou
         }
     }
 #pragma unroll
-    for (int k = 0; k < 16; k++) s[k << LS] = v[k];
+    for (int k = 0; k < 16; k++) s[r16_off<LS, PADL>(k)] = v[k];
+}
+
+// Radix-16 round on padded single-column tiles (the last pass: C = 1, Qb = 1,
+// j0 = 0), any tile count (k_pwr's a/b tiles of one or both primes): unit
+// (block b, row j2 < q16 = 2^LS) holds rows 16 q16 b + j2 + k q16.  With
+// j2 < q16 <= 16 or q16 a multiple of 16, the padded offset of point k is
+// lay(first point) + r16_off<LS, true>(k): compile-time.
+template <bool FWD, int LS>
+__device__ NBG_ROUND void round_r16_c1(const Tiles& T, const DStage& A, const DStage& B) {
+    const int per = T.G >> 4;
+    const int total = per * T.ntiles;
+    const uint32_t QA = (uint32_t)A.Q, QB = (uint32_t)B.Q;
+    const uint32_t stepA = 1u << LS;
+    const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
+    const double *twA0 = A.tw[0], *twA1 = A.tw[1], *twB0 = B.tw[0], *twB1 = B.tw[1];
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        int tau;
+        const int r = split_unit(u, per, tau);
+        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : (tau >> T.pshift) != 0;
+        const int b = r >> LS, j2 = r & ((1 << LS) - 1);
+        double* su = T.s + tau * T.stride + sp((b << (LS + 4)) + j2);
+        if (p1) r16_unit_dense<FWD, LS, 1, true>(su, twA1 + j2, twB1 + j2, stepA, QA, QB, wi1);
+        else r16_unit_dense<FWD, LS, 0, true>(su, twA0 + j2, twB0 + j2, stepA, QA, QB, wi0);
+    }
+}
+
+template <bool FWD>
+__device__ __forceinline__ void round_r16_c1_any(const Tiles& T, const DStage& A, const DStage& B) {
+    switch (__ffs((int)A.L) - 1 - 4) {  // log2(q16)
+        case 0: round_r16_c1<FWD, 0>(T, A, B); break;
+        case 1: round_r16_c1<FWD, 1>(T, A, B); break;
+        case 2: round_r16_c1<FWD, 2>(T, A, B); break;
+        case 3: round_r16_c1<FWD, 3>(T, A, B); break;
+        case 4: round_r16_c1<FWD, 4>(T, A, B); break;
+        case 5: round_r16_c1<FWD, 5>(T, A, B); break;
+        case 6: round_r16_c1<FWD, 6>(T, A, B); break;
+        case 7: round_r16_c1<FWD, 7>(T, A, B); break;
+        case 8: round_r16_c1<FWD, 8>(T, A, B); break;
+        default: round_r16<FWD, true>(T, A, B); break;
+    }
 }
 
 // Tiles: prime 0 at T.s, prime 1 at T.s + T.stride (dense, row length C = 2^lc).
@@ -537,8 +584,10 @@ __device__ void run_round(const Tiles& T, const DPlan& pl, int kind, int s0) {
     const DStage& st = pl.st[s0];
     switch (kind) {
         case RK_R16:
-            if (PAD) round_r16<FWD, PAD>(T, st, pl.st[s0 + 1]);
-            else round_r16_dense_any<FWD>(T, st, pl.st[s0 + 1]);
+            if (!PAD) round_r16_dense_any<FWD>(T, st, pl.st[s0 + 1]);
+            else if (T.lc == 0 && T.Qb == 1 && T.j0 == 0 && (st.L & (st.L - 1)) == 0)
+                round_r16_c1_any<FWD>(T, st, pl.st[s0 + 1]);
+            else round_r16<FWD, PAD>(T, st, pl.st[s0 + 1]);
             break;
         case RK_R4: round_gen<4, FWD, PAD>(T, st); break;
         case RK_R8:
@@ -934,59 +983,32 @@ __device__ __forceinline__ void tile_box(const DPass& ps, int64_t t, int& x, int
     y = (int)(blk * ps.G);
 }
 
-// One column pass (forward or reverse) of a run of tiles, staged by TMA and
-// pipelined by prime.  A CTA walks its jobs as half-jobs h = (job, prime) with
-// one shared-memory buffer per prime: at the start of half-job h, thread 0
-// waits until the store of half-job h - 1 has read its buffer and issues the
-// load of half-job h + 1 into it, so that load runs while half-job h is
-// transformed.  Dynamic shared memory: [2 mbarriers | 112 B | buffer 0 |
-// buffer 1], each buffer one G x C tile.  Pass 0 of a forward transform packs
-// limbs instead of loading: the pack is written into both buffers at the
-// job's first half (both tiles hold the same chunks).
+// One column pass (forward or reverse), staged by TMA, one prime's tile per
+// CTA step: a CTA of COL_THREADS threads walks a run of consecutive half-jobs
+// h = (job h / 2, prime h % 2).  Small CTAs with one tile each let six CTAs
+// share an SM (80 registers, about 33 KB of shared memory each), so a CTA
+// waiting for its tile's load leaves five that compute.  Thread 0 issues one
+// cp.async.bulk.tensor load of the tile (completing on an mbarrier) and, after
+// the rounds, one store; the next load waits until that store has read shared
+// memory.  Dynamic shared memory: [mbarrier | 120 B | tile].  Forward pass 0
+// packs the prime's tile from the limbs instead of loading it.
+constexpr int COL_THREADS = 128;
+
 template <int MINB, bool FWD, bool ODD>
-__global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __restrict__ prods,
-                                                             const DPlan* __restrict__ plans,
-                                                             const Job* __restrict__ jobs, int64_t njobs) {
+__global__ void __launch_bounds__(COL_THREADS, MINB) k_col_tma(const DProd* __restrict__ prods,
+                                                            const DPlan* __restrict__ plans,
+                                                            const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ __align__(128) double dsm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm);  // bar[0], bar[1]
-    double* smem = dsm + 16;                           // buffers start 128 bytes in
-    if (threadIdx.x == 0) {
-        tma::bar_init(bar);
-        tma::bar_init(bar + 1);
-    }
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm);
+    double* smem = dsm + 16;  // the tile starts 128 bytes in
+    if (threadIdx.x == 0) tma::bar_init(bar);
     __syncthreads();
-    uint32_t phase[2] = {0, 0};
-    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
-    const int64_t j0 = (int64_t)blockIdx.x * run;
-    const int64_t jend = min(njobs, j0 + run);
-    if (j0 >= jend) return;
-    const int64_t nhalf = 2 * (jend - j0);
-    // every job of a launch has the same tile size
-    int cnt;
-    {
-        const Job jb = jobs[j0];
-        const DPass& ps = plans[prods[jb.prod].plan].pass[(jb.sub >> 8) & 0xff];
-        cnt = ps.G * ps.C;
-    }
-    // issues the load of half-job h (thread 0), unless its job packs limbs
-    auto issue = [&](int64_t h) {
-        const Job jb = jobs[j0 + (h >> 1)];
-        const int f = (int)(h & 1);
-        const DProd& P = prods[jb.prod];
-        const int pass = (jb.sub >> 8) & 0xff;
-        if (FWD && pass == 0 && !(P.flags & PF_PRELOADED)) return;
-        const int opb = FWD ? (jb.sub >> 1) & 1 : 0;
-        const DPass& ps = plans[P.plan].pass[pass];
-        int x, y;
-        tile_box(ps, jb.tile, x, y);
-        const void* map = static_cast<const char*>(P.tmap) + 128 * (2 * pass + opb);
-        tma::fence_map(map);
-        tma::bar_expect(bar + f, (uint32_t)(cnt * sizeof(double)));
-        tma::load3(smem + f * cnt, map, x, y, 2 * P.tslot + f, bar + f);
-    };
-    if (threadIdx.x == 0) issue(0);
-    for (int64_t h = 0; h < nhalf; h++) {
-        const Job jb = jobs[j0 + (h >> 1)];
+    uint32_t phase = 0;
+    const int64_t nh = 2 * njobs;
+    const int64_t run = (nh + gridDim.x - 1) / gridDim.x;
+    const int64_t hend = min(nh, ((int64_t)blockIdx.x + 1) * run);
+    for (int64_t h = (int64_t)blockIdx.x * run; h < hend; h++) {
+        const Job jb = jobs[h >> 1];
         const int f = (int)(h & 1);
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
@@ -995,34 +1017,37 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __r
         const DPass& ps = pl.pass[pass];
         int x, y;
         tile_box(ps, jb.tile, x, y);
+        const int z = 2 * P.tslot + f;
         const void* map = static_cast<const char*>(P.tmap) + 128 * (2 * pass + opb);
+        const int cnt = ps.G * ps.C;
         const bool pack = FWD && pass == 0 && !(P.flags & PF_PRELOADED);
-        double* buf = smem + f * cnt;
-        __syncthreads();  // every thread is done with half-job h - 1
+        __syncthreads();  // every thread is done with the previous tile
         if (threadIdx.x == 0) {
-            tma::stores_read();  // the store of half-job h - 1 has read its buffer
-            if (h + 1 < nhalf) issue(h + 1);
+            tma::stores_read();  // the previous tile's store has read shared memory
+            if (!pack) {
+                tma::fence_map(map);
+                tma::bar_expect(bar, (uint32_t)(cnt * sizeof(double)));
+                tma::load3(smem, map, x, y, z, bar);
+            }
         }
         if (pack) {
-            if (f == 0) {  // both primes' tiles hold the same chunks
-                __syncthreads();
-                const int64_t base = (int64_t)(y / ps.G) * pl.st[ps.sa].L + x;
-                if (opb) pack_tile2<false>(smem, smem + cnt, P.b, P.n, P.bch, P.ncb, ps, base);
-                else pack_tile2<false>(smem, smem + cnt, P.a, P.m, P.bch, P.nca, ps, base);
-            }
+            __syncthreads();
+            const int64_t base = (int64_t)(y / ps.G) * pl.st[ps.sa].L + x;
+            if (opb) pack_tile2<false>(smem, smem, P.b, P.n, P.bch, P.ncb, ps, base);
+            else pack_tile2<false>(smem, smem, P.a, P.m, P.bch, P.nca, ps, base);
         } else {
-            if (!tma::bar_wait(bar + f, phase[f])) {  // gave up: leave after the stores issued so far
+            if (!tma::bar_wait(bar, phase)) {  // gave up: leave after the stores issued so far
                 if (threadIdx.x == 0) tma::stores_done();
                 return;
             }
-            phase[f] ^= 1u;
+            phase ^= 1u;
         }
-        Tiles T = make_tiles(buf, cnt, 1, 30, ps, x);
+        Tiles T = make_tiles(smem, cnt, 1, 30, ps, x);
         T.pfix = f;
         run_pass<FWD, false, ODD>(T, pl, ps);
         tma::fence_async();
         __syncthreads();
-        if (threadIdx.x == 0) tma::store3(map, x, y, 2 * P.tslot + f, buf);
+        if (threadIdx.x == 0) tma::store3(map, x, y, z, smem);
     }
     if (threadIdx.x == 0) tma::stores_done();
 }
@@ -1413,10 +1438,8 @@ cudaError_t kernels_init(double p1, double p2) {
                         (const void*)k_pwr<true, false, false>, (const void*)k_pwr<false, true, false>,
                         (const void*)k_rev<3, true>, (const void*)k_rev<4, true>, (const void*)k_rev<3, false>,
                         (const void*)k_rev<4, false>, (const void*)k_unpack,
-                        (const void*)k_col_tma<3, true, true>, (const void*)k_col_tma<4, true, true>,
-                        (const void*)k_col_tma<3, false, true>, (const void*)k_col_tma<4, false, true>,
-                        (const void*)k_col_tma<3, true, false>, (const void*)k_col_tma<4, true, false>,
-                        (const void*)k_col_tma<3, false, false>, (const void*)k_col_tma<4, false, false>};
+                        (const void*)k_col_tma<6, true, true>, (const void*)k_col_tma<6, false, true>,
+                        (const void*)k_col_tma<6, true, false>, (const void*)k_col_tma<6, false, false>};
     for (const void* k : ks) {
         cudaFuncAttributes fa;
         e = cudaFuncGetAttributes(&fa, k);
@@ -1465,22 +1488,30 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
         if (odd) KERNEL<__VA_ARGS__, true><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);   \
         else KERNEL<__VA_ARGS__, false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);      \
     } while (0)
-    const bool c4 = smem <= COL4_MAX_SMEM, c4t = smem <= COL4_MAX_SMEM_TMA;
+    const bool c4 = smem <= COL4_MAX_SMEM;
     switch (kind) {
         case JK_FWD:
             if (c4) NBG_ODD(k_fwd, 4);
             else NBG_ODD(k_fwd, 3);
             break;
-        // passes with radix-3/5/7 rounds take the 80-register build whatever
-        // their tile size (the 64-register one spills there)
+        // one prime's tile per CTA step: 2 * njobs half-jobs, runs of up to 8
+        // consecutive ones per CTA while keeping >= 4 waves of 6 CTAs per SM
         case JK_FWD_TMA:
-            if (c4t && !odd) NBG_ODD(k_col_tma, 4, true);
-            else NBG_ODD(k_col_tma, 3, true);
+        case JK_REV_TMA: {
+            const int64_t nh = 2 * njobs;
+            const int64_t k = std::max<int64_t>(1, std::min<int64_t>(8, nh / (148 * 6 * 4)));
+            int64_t g = (nh + k - 1) / k;
+            if (grid_cap > 0 && g > grid_cap) g = grid_cap;
+            const unsigned gt = (unsigned)std::min<int64_t>(g, 0x7fffffff);
+            if (kind == JK_FWD_TMA) {
+                if (odd) k_col_tma<6, true, true><<<gt, COL_THREADS, smem, st>>>(prods, plans, jobs, njobs);
+                else k_col_tma<6, true, false><<<gt, COL_THREADS, smem, st>>>(prods, plans, jobs, njobs);
+            } else {
+                if (odd) k_col_tma<6, false, true><<<gt, COL_THREADS, smem, st>>>(prods, plans, jobs, njobs);
+                else k_col_tma<6, false, false><<<gt, COL_THREADS, smem, st>>>(prods, plans, jobs, njobs);
+            }
             break;
-        case JK_REV_TMA:
-            if (c4t && !odd) NBG_ODD(k_col_tma, 4, false);
-            else NBG_ODD(k_col_tma, 3, false);
-            break;
+        }
         case JK_PWR: NBG_ODD(k_pwr, false, false); break;
         case JK_PWR_SPLIT: NBG_ODD(k_pwr, true, false); break;
         case JK_PWR_KEEP: NBG_ODD(k_pwr, false, true); break;

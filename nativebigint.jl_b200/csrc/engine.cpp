@@ -710,13 +710,13 @@ static bool tma_pass_ok(const DPass& ps) {
 }
 
 // The 3-D map over nbuf transform buffers of N doubles at base: dims (Qb, N/Qb,
-// nbuf), box (C, G, 1): one box is one prime's tile of one product.
+// nbuf), box (C, G, 2): one box is one tile of both primes of one product.
 static int encode_pass_map(void* out, double* base, int64_t N, int64_t nbuf, const DPass& ps) {
     auto enc = tma_encoder();
     if (!enc) return fail(NBG_ECUDA, "cuTensorMapEncodeTiled unavailable");
     const cuuint64_t dims[3] = {(cuuint64_t)ps.Qb, (cuuint64_t)(N / ps.Qb), (cuuint64_t)nbuf};
     const cuuint64_t strides[2] = {(cuuint64_t)ps.Qb * sizeof(double), (cuuint64_t)N * sizeof(double)};
-    const cuuint32_t box[3] = {(cuuint32_t)ps.C, (cuuint32_t)ps.G, 1};
+    const cuuint32_t box[3] = {(cuuint32_t)ps.C, (cuuint32_t)ps.G, 2};
     const cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box,
                      estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -911,7 +911,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         for (int p = 0; p < Pn - 1; p++) {
             const DPass& ps = pl.pass[p];
             const bool tp = (tmask >> p) & 1u;
-            const size_t smem = tp ? 128 + sizeof(double) * (size_t)(ps.G * ps.C)
+            const size_t smem = tp ? 128 + sizeof(double) * 2 * (size_t)(ps.G * ps.C)
                                    : sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
             const double jobs = (double)ps.ntiles * nop * nc;
@@ -941,7 +941,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         for (int p = Pn - 2; p >= 0; p--) {
             const DPass& ps = pl.pass[p];
             const bool tp = (tmask >> p) & 1u;
-            const size_t smem = tp ? 128 + sizeof(double) * (size_t)(ps.G * ps.C)
+            const size_t smem = tp ? 128 + sizeof(double) * 2 * (size_t)(ps.G * ps.C)
                                    : sizeof(double) * 2 * (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
             const double jobs = (double)ps.ntiles * nc;

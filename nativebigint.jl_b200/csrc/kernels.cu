@@ -38,6 +38,7 @@
 #endif
 // Column passes with tile sets up to this size run the 4-CTA/SM build.
 constexpr size_t COL4_MAX_SMEM = 32 * 1024;
+constexpr size_t COL4_MAX_SMEM_TMA = 32 * 1024 + 128;  // the TMA tiles plus their mbarrier line
 // Rounds are inlined into the kernels; out-of-line rounds (NBG_ROUND_NOINLINE)
 // measured 40% slower in k_pwr.
 #ifdef NBG_ROUND_NOINLINE
@@ -248,22 +249,14 @@ __device__ __forceinline__ void bf4(double& a, double& b, double& c, double& d, 
     if (!FWD) dft4(a, b, c, d, wi, F);
 }
 
-// Offset of a unit's point k from its point 0: 2^LS elements apart, or on a
-// padded tile (one double in 16) with single columns, where the unit's first
-// point sits below a multiple of 2^LS + ... so the padding adds (k 2^LS) / 16.
-template <int LS, bool PADL>
-__device__ __forceinline__ constexpr int r16_off(int k) {
-    return PADL ? (k << LS) + ((k << LS) >> 4) : (k << LS);
-}
-
-template <bool FWD, int LS, int PR, bool PADL = false>
+template <bool FWD, int LS, int PR>
 __device__ __forceinline__ void r16_unit_dense(double* __restrict__ s, const double* __restrict__ twA,
                                                const double* __restrict__ twB, uint32_t stepA, uint32_t QA,
                                                uint32_t QB, double wi) {
     const Fp F = c_fp[PR];
     double v[16];
 #pragma unroll
-    for (int k = 0; k < 16; k++) v[k] = s[r16_off<LS, PADL>(k)];
+    for (int k = 0; k < 16; k++) v[k] = s[k << LS];
     if (FWD) {
 #pragma unroll
         for (int t2 = 0; t2 < 4; t2++) {
@@ -286,47 +279,7 @@ __device__ __forceinline__ void r16_unit_dense(double* __restrict__ s, const dou
         }
     }
 #pragma unroll
-    for (int k = 0; k < 16; k++) s[r16_off<LS, PADL>(k)] = v[k];
-}
-
-// Radix-16 round on padded single-column tiles (the last pass: C = 1, Qb = 1,
-// j0 = 0), any tile count (k_pwr's a/b tiles of one or both primes): unit
-// (block b, row j2 < q16 = 2^LS) holds rows 16 q16 b + j2 + k q16.  With
-// j2 < q16 <= 16 or q16 a multiple of 16, the padded offset of point k is
-// lay(first point) + r16_off<LS, true>(k): compile-time.
-template <bool FWD, int LS>
-__device__ NBG_ROUND void round_r16_c1(const Tiles& T, const DStage& A, const DStage& B) {
-    const int per = T.G >> 4;
-    const int total = per * T.ntiles;
-    const uint32_t QA = (uint32_t)A.Q, QB = (uint32_t)B.Q;
-    const uint32_t stepA = 1u << LS;
-    const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
-    const double *twA0 = A.tw[0], *twA1 = A.tw[1], *twB0 = B.tw[0], *twB1 = B.tw[1];
-    for (int u = threadIdx.x; u < total; u += blockDim.x) {
-        int tau;
-        const int r = split_unit(u, per, tau);
-        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : (tau >> T.pshift) != 0;
-        const int b = r >> LS, j2 = r & ((1 << LS) - 1);
-        double* su = T.s + tau * T.stride + sp((b << (LS + 4)) + j2);
-        if (p1) r16_unit_dense<FWD, LS, 1, true>(su, twA1 + j2, twB1 + j2, stepA, QA, QB, wi1);
-        else r16_unit_dense<FWD, LS, 0, true>(su, twA0 + j2, twB0 + j2, stepA, QA, QB, wi0);
-    }
-}
-
-template <bool FWD>
-__device__ __forceinline__ void round_r16_c1_any(const Tiles& T, const DStage& A, const DStage& B) {
-    switch (__ffs((int)A.L) - 1 - 4) {  // log2(q16)
-        case 0: round_r16_c1<FWD, 0>(T, A, B); break;
-        case 1: round_r16_c1<FWD, 1>(T, A, B); break;
-        case 2: round_r16_c1<FWD, 2>(T, A, B); break;
-        case 3: round_r16_c1<FWD, 3>(T, A, B); break;
-        case 4: round_r16_c1<FWD, 4>(T, A, B); break;
-        case 5: round_r16_c1<FWD, 5>(T, A, B); break;
-        case 6: round_r16_c1<FWD, 6>(T, A, B); break;
-        case 7: round_r16_c1<FWD, 7>(T, A, B); break;
-        case 8: round_r16_c1<FWD, 8>(T, A, B); break;
-        default: round_r16<FWD, true>(T, A, B); break;
-    }
+    for (int k = 0; k < 16; k++) s[k << LS] = v[k];
 }
 
 // Tiles: prime 0 at T.s, prime 1 at T.s + T.stride (dense, row length C = 2^lc).
@@ -341,18 +294,15 @@ __device__ NBG_ROUND void round_r16_dense(const Tiles& T, const DStage& A, const
     const uint32_t stepA = (uint32_t)q16 * (uint32_t)T.Qb;
     const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
     const double *twA0 = A.tw[0], *twA1 = A.tw[1], *twB0 = B.tw[0], *twB1 = B.tw[1];
-    // pfix >= 0: the tiles hold that prime alone (at T.s)
-    const int total = T.pfix >= 0 ? per : 2 * per;
-    double* const s1 = T.pfix >= 0 ? T.s : T.s + T.stride;
-    for (int u = threadIdx.x; u < total; u += blockDim.x) {
-        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : u >= per;
-        const int uu = (T.pfix < 0 && p1) ? u - per : u;
+    for (int u = threadIdx.x; u < 2 * per; u += blockDim.x) {
+        const bool p1 = u >= per;
+        const int uu = p1 ? u - per : u;
         const int c = uu & (C - 1);
         const int r = uu >> lc;
         const int b = r >> lq, j2 = r & (q16 - 1);
         const int base = ((b * Lloc + j2) << lc) + c;
         const uint32_t jB = (uint32_t)j2 * (uint32_t)T.Qb + (uint32_t)(T.j0 + c);
-        if (p1) r16_unit_dense<FWD, LS, 1>(s1 + base, twA1 + jB, twB1 + jB, stepA, QA, QB, wi1);
+        if (p1) r16_unit_dense<FWD, LS, 1>(T.s + T.stride + base, twA1 + jB, twB1 + jB, stepA, QA, QB, wi1);
         else r16_unit_dense<FWD, LS, 0>(T.s + base, twA0 + jB, twB0 + jB, stepA, QA, QB, wi0);
     }
 }
@@ -584,10 +534,8 @@ __device__ void run_round(const Tiles& T, const DPlan& pl, int kind, int s0) {
     const DStage& st = pl.st[s0];
     switch (kind) {
         case RK_R16:
-            if (!PAD) round_r16_dense_any<FWD>(T, st, pl.st[s0 + 1]);
-            else if (T.lc == 0 && T.Qb == 1 && T.j0 == 0 && (st.L & (st.L - 1)) == 0)
-                round_r16_c1_any<FWD>(T, st, pl.st[s0 + 1]);
-            else round_r16<FWD, PAD>(T, st, pl.st[s0 + 1]);
+            if (PAD) round_r16<FWD, PAD>(T, st, pl.st[s0 + 1]);
+            else round_r16_dense_any<FWD>(T, st, pl.st[s0 + 1]);
             break;
         case RK_R4: round_gen<4, FWD, PAD>(T, st); break;
         case RK_R8:
@@ -983,33 +931,22 @@ __device__ __forceinline__ void tile_box(const DPass& ps, int64_t t, int& x, int
     y = (int)(blk * ps.G);
 }
 
-// One column pass (forward or reverse), staged by TMA, one prime's tile per
-// CTA step: a CTA of COL_THREADS threads walks a run of consecutive half-jobs
-// h = (job h / 2, prime h % 2).  Small CTAs with one tile each let six CTAs
-// share an SM (80 registers, about 33 KB of shared memory each), so a CTA
-// waiting for its tile's load leaves five that compute.  Thread 0 issues one
-// cp.async.bulk.tensor load of the tile (completing on an mbarrier) and, after
-// the rounds, one store; the next load waits until that store has read shared
-// memory.  Dynamic shared memory: [mbarrier | 120 B | tile].  Forward pass 0
-// packs the prime's tile from the limbs instead of loading it.
-constexpr int COL_THREADS = 128;
-
+// One column pass (forward or reverse) of one tile of one operand, both primes,
+// staged by TMA.  Dynamic shared memory: [mbarrier | 120 B | tiles].
 template <int MINB, bool FWD, bool ODD>
-__global__ void __launch_bounds__(COL_THREADS, MINB) k_col_tma(const DProd* __restrict__ prods,
-                                                            const DPlan* __restrict__ plans,
-                                                            const Job* __restrict__ jobs, int64_t njobs) {
+__global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __restrict__ prods,
+                                                             const DPlan* __restrict__ plans,
+                                                             const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ __align__(128) double dsm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(dsm);
-    double* smem = dsm + 16;  // the tile starts 128 bytes in
+    double* smem = dsm + 16;  // tiles start 128 bytes in
     if (threadIdx.x == 0) tma::bar_init(bar);
     __syncthreads();
     uint32_t phase = 0;
-    const int64_t nh = 2 * njobs;
-    const int64_t run = (nh + gridDim.x - 1) / gridDim.x;
-    const int64_t hend = min(nh, ((int64_t)blockIdx.x + 1) * run);
-    for (int64_t h = (int64_t)blockIdx.x * run; h < hend; h++) {
-        const Job jb = jobs[h >> 1];
-        const int f = (int)(h & 1);
+    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
+    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
+    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
+        const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int opb = FWD ? (jb.sub >> 1) & 1 : 0;
@@ -1017,7 +954,7 @@ __global__ void __launch_bounds__(COL_THREADS, MINB) k_col_tma(const DProd* __re
         const DPass& ps = pl.pass[pass];
         int x, y;
         tile_box(ps, jb.tile, x, y);
-        const int z = 2 * P.tslot + f;
+        const int z = 2 * P.tslot;
         const void* map = static_cast<const char*>(P.tmap) + 128 * (2 * pass + opb);
         const int cnt = ps.G * ps.C;
         const bool pack = FWD && pass == 0 && !(P.flags & PF_PRELOADED);
@@ -1026,15 +963,15 @@ __global__ void __launch_bounds__(COL_THREADS, MINB) k_col_tma(const DProd* __re
             tma::stores_read();  // the previous tile's store has read shared memory
             if (!pack) {
                 tma::fence_map(map);
-                tma::bar_expect(bar, (uint32_t)(cnt * sizeof(double)));
+                tma::bar_expect(bar, (uint32_t)(2 * cnt * sizeof(double)));
                 tma::load3(smem, map, x, y, z, bar);
             }
         }
         if (pack) {
             __syncthreads();
             const int64_t base = (int64_t)(y / ps.G) * pl.st[ps.sa].L + x;
-            if (opb) pack_tile2<false>(smem, smem, P.b, P.n, P.bch, P.ncb, ps, base);
-            else pack_tile2<false>(smem, smem, P.a, P.m, P.bch, P.nca, ps, base);
+            if (opb) pack_tile2<false>(smem, smem + cnt, P.b, P.n, P.bch, P.ncb, ps, base);
+            else pack_tile2<false>(smem, smem + cnt, P.a, P.m, P.bch, P.nca, ps, base);
         } else {
             if (!tma::bar_wait(bar, phase)) {  // gave up: leave after the stores issued so far
                 if (threadIdx.x == 0) tma::stores_done();
@@ -1042,9 +979,7 @@ __global__ void __launch_bounds__(COL_THREADS, MINB) k_col_tma(const DProd* __re
             }
             phase ^= 1u;
         }
-        Tiles T = make_tiles(smem, cnt, 1, 30, ps, x);
-        T.pfix = f;
-        run_pass<FWD, false, ODD>(T, pl, ps);
+        run_pass<FWD, false, ODD>(make_tiles(smem, cnt, 2, 0, ps, x), pl, ps);
         tma::fence_async();
         __syncthreads();
         if (threadIdx.x == 0) tma::store3(map, x, y, z, smem);
@@ -1438,8 +1373,10 @@ cudaError_t kernels_init(double p1, double p2) {
                         (const void*)k_pwr<true, false, false>, (const void*)k_pwr<false, true, false>,
                         (const void*)k_rev<3, true>, (const void*)k_rev<4, true>, (const void*)k_rev<3, false>,
                         (const void*)k_rev<4, false>, (const void*)k_unpack,
-                        (const void*)k_col_tma<6, true, true>, (const void*)k_col_tma<6, false, true>,
-                        (const void*)k_col_tma<6, true, false>, (const void*)k_col_tma<6, false, false>};
+                        (const void*)k_col_tma<3, true, true>, (const void*)k_col_tma<4, true, true>,
+                        (const void*)k_col_tma<3, false, true>, (const void*)k_col_tma<4, false, true>,
+                        (const void*)k_col_tma<3, true, false>, (const void*)k_col_tma<4, true, false>,
+                        (const void*)k_col_tma<3, false, false>, (const void*)k_col_tma<4, false, false>};
     for (const void* k : ks) {
         cudaFuncAttributes fa;
         e = cudaFuncGetAttributes(&fa, k);
@@ -1488,30 +1425,22 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
         if (odd) KERNEL<__VA_ARGS__, true><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);   \
         else KERNEL<__VA_ARGS__, false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);      \
     } while (0)
-    const bool c4 = smem <= COL4_MAX_SMEM;
+    const bool c4 = smem <= COL4_MAX_SMEM, c4t = smem <= COL4_MAX_SMEM_TMA;
     switch (kind) {
         case JK_FWD:
             if (c4) NBG_ODD(k_fwd, 4);
             else NBG_ODD(k_fwd, 3);
             break;
-        // one prime's tile per CTA step: 2 * njobs half-jobs, runs of up to 8
-        // consecutive ones per CTA while keeping >= 4 waves of 6 CTAs per SM
+        // passes with radix-3/5/7 rounds take the 80-register build whatever
+        // their tile size (the 64-register one spills there)
         case JK_FWD_TMA:
-        case JK_REV_TMA: {
-            const int64_t nh = 2 * njobs;
-            const int64_t k = std::max<int64_t>(1, std::min<int64_t>(8, nh / (148 * 6 * 4)));
-            int64_t g = (nh + k - 1) / k;
-            if (grid_cap > 0 && g > grid_cap) g = grid_cap;
-            const unsigned gt = (unsigned)std::min<int64_t>(g, 0x7fffffff);
-            if (kind == JK_FWD_TMA) {
-                if (odd) k_col_tma<6, true, true><<<gt, COL_THREADS, smem, st>>>(prods, plans, jobs, njobs);
-                else k_col_tma<6, true, false><<<gt, COL_THREADS, smem, st>>>(prods, plans, jobs, njobs);
-            } else {
-                if (odd) k_col_tma<6, false, true><<<gt, COL_THREADS, smem, st>>>(prods, plans, jobs, njobs);
-                else k_col_tma<6, false, false><<<gt, COL_THREADS, smem, st>>>(prods, plans, jobs, njobs);
-            }
+            if (c4t && !odd) NBG_ODD(k_col_tma, 4, true);
+            else NBG_ODD(k_col_tma, 3, true);
             break;
-        }
+        case JK_REV_TMA:
+            if (c4t && !odd) NBG_ODD(k_col_tma, 4, false);
+            else NBG_ODD(k_col_tma, 3, false);
+            break;
         case JK_PWR: NBG_ODD(k_pwr, false, false); break;
         case JK_PWR_SPLIT: NBG_ODD(k_pwr, true, false); break;
         case JK_PWR_KEEP: NBG_ODD(k_pwr, false, true); break;

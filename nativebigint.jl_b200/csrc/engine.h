@@ -36,7 +36,7 @@ struct Tuning {
     int last_max = 2048;      // largest contiguous block of the last pass, products
     int last_max_sqr = 4096;  // same for squares
     int early_gmax = 256;     // largest row count of an early (column) pass
-    int tile_target = 2048;   // target doubles per column-pass tile
+    int tile_target = 4096;   // target doubles per column-pass tile (>= 16 G: TMA-eligible columns)
     int cmax = 128;           // most adjacent columns per column-pass tile
     int tma = 1;              // stage column tiles of at least 16 columns by TMA (0: cp.async for all)
     std::map<int64_t, SplitOverride> overrides;  // key: N * 2 + square

@@ -43,7 +43,9 @@ def _fits_last(L: int, sqr: bool) -> bool:
 def candidates(N: int, sqr: bool, tile_targets=None) -> list[dict]:
     """Pass splits (last stage of each pass) worth timing for class (N, sqr)."""
     if tile_targets is None:
-        tile_targets = (2048,) if N >= 1 << 22 else (1024, 2048, 4096)
+        # column tiles of at least 16 columns are staged by TMA: G <= 256 rows
+        # need a target of 4096 points for that
+        tile_targets = (4096,) if N >= 1 << 22 else (2048, 4096, 8192)
     st = plan_layout(N, sqr)["stages"]
     S = len(st)
     out = []

@@ -1256,41 +1256,32 @@ __global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, 
 }
 
 // Tiles that k_carry flagged (bit 2 of their aggregate): the incoming carry
-// runs through the tile's leading all-ones limbs.  For each flagged tile the
-// whole block finds the first limb that is not all ones (it absorbs the +1),
-// zeroing the run before it; a tile that is all ones passes the carry on,
-// which the cross-tile scan already credited to the next tile.  Jobs are the
-// unpack's (product, tile) list, checked 256 at a time (one per thread).
+// runs through the tile's leading all-ones limbs.  One warp per tile: an
+// unflagged tile is left at once; a flagged one is read 32 limbs at a time
+// until the first limb that is not all ones (it absorbs the +1), the run before
+// it zeroed; a tile that is all ones passes the carry on, which the cross-tile
+// scan already credited to the next tile.  Jobs are the unpack's (product,
+// tile) list.
 __global__ void __launch_bounds__(256) k_carry_fix(const DProd* __restrict__ prods, const Job* __restrict__ jobs,
                                                    int64_t njobs) {
-    __shared__ unsigned long long first;
-    __shared__ int nflag;
-    __shared__ int64_t flagged[256];
-    // the block checks 256 tiles at once (one per thread) and walks the flagged ones
-    for (int64_t j0 = (int64_t)blockIdx.x * blockDim.x; j0 < njobs; j0 += (int64_t)gridDim.x * blockDim.x) {
-        if (threadIdx.x == 0) nflag = 0;
-        __syncthreads();
-        const int64_t ji = j0 + threadIdx.x;
-        if (ji < njobs) {
-            const Job jb = jobs[ji];
-            const DProd& P = prods[jb.prod];
-            if (P.ntl > 1 && (P.agg[jb.tile] & 4u)) flagged[atomicAdd(&nflag, 1)] = ji;
-        }
-        __syncthreads();
-        const int nf = nflag;
-        for (int f = 0; f < nf; f++) {
-            const Job jb = jobs[flagged[f]];
-            const DProd& P = prods[jb.prod];
-            const int64_t w0 = jb.tile * UNPACK_TL, we = min(w0 + (int64_t)UNPACK_TL, P.rn);
-            if (threadIdx.x == 0) first = (unsigned long long)we;
-            __syncthreads();
-            for (int64_t w = w0 + threadIdx.x; w < we; w += blockDim.x)
-                if (P.r[w] != ~0ULL) atomicMin(&first, (unsigned long long)w);
-            __syncthreads();
-            const int64_t fw = (int64_t)first;
-            for (int64_t w = w0 + threadIdx.x; w < fw; w += blockDim.x) P.r[w] = 0;
-            if (threadIdx.x == 0 && fw < we) P.r[fw] += 1;
-            __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t ji = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); ji < njobs; ji += nw) {
+        const Job jb = jobs[ji];
+        const DProd& P = prods[jb.prod];
+        if (P.ntl <= 1 || !(P.agg[jb.tile] & 4u)) continue;
+        const int64_t w0 = jb.tile * UNPACK_TL, we = min(w0 + (int64_t)UNPACK_TL, P.rn);
+        for (int64_t w = w0; w < we; w += 32) {
+            const int64_t wl = w + lane;
+            const uint64_t v = wl < we ? P.r[wl] : 0ULL;  // past the tile: stops the run
+            const unsigned notones = __ballot_sync(0xffffffffu, v != ~0ULL);
+            if (notones) {
+                const int k = __ffs(notones) - 1;
+                if (lane < k) P.r[wl] = 0;
+                else if (lane == k && wl < we) P.r[wl] = v + 1;
+                break;
+            }
+            P.r[wl] = 0;  // all 32 are all ones (and inside the tile)
         }
     }
 }
@@ -1451,8 +1442,8 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
         case JK_UNPACK: k_unpack<<<grid, UNPACK_THREADS, smem, st>>>(prods, plans, jobs, njobs); break;
         case JK_CARRY: k_carry<<<grid, 256, 0, st>>>(prods, jobs, njobs); break;
         case JK_CARRYFIX: {
-            // each block checks 256 tiles per step; most tiles are skipped
-            const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((njobs + 255) / 256, 148 * 8));
+            // one warp per tile (most tiles are left at once)
+            const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((njobs + 7) / 8, 148 * 32));
             k_carry_fix<<<g, 256, 0, st>>>(prods, jobs, njobs);
             break;
         }

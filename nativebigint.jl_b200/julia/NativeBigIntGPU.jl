@@ -161,14 +161,17 @@ function gpu_radix_powtab(bb::Limb, x::Vector{Limb})
 end
 
 # Per-call crossover of the drop-in hook: one host-buffer call (pageable
-# Memory, copies included) against the reference's CPU engine.  A product goes
-# to the GPU when its smaller operand has at least GPU_MIN_LIMBS limbs (squares:
-# GPU_MIN_SQR_LIMBS); smaller NTT-sized products keep the reference's CPU
-# mul_fpntt2!/sqr_fpntt2!.  Measured with bench.py --route (route_crossover:
-# GPU call vs GMP on one core x the reference's published mul!/mpn_mul ratio).
-const GPU_MIN_LIMBS = Ref(4864)
-const GPU_MIN_SQR_LIMBS = Ref(4864)
-gpu_pays(m::Int, n::Int) = min(m, n) >= GPU_MIN_LIMBS[]
+# Memory, copies included) against the reference's CPU engine.  Measured on
+# B200 with bench.py --route (route_crossover: the GPU call against GMP on one
+# host core times the reference's published mul!/mpn_mul ratio): a call costs
+# 58 us at 152 limbs and 109 us at 4864; it overtakes the CPU engine near
+# m + n = 5200 output limbs for balanced products, 3950 for m = 4n, and
+# n = 3260 for squares.  Products at or above GPU_MIN_OUT_LIMBS output limbs
+# (squares: GPU_MIN_SQR_LIMBS operand limbs) go to the GPU; smaller NTT-sized
+# products keep the reference's CPU mul_fpntt2!/sqr_fpntt2!.
+const GPU_MIN_OUT_LIMBS = Ref(4600)
+const GPU_MIN_SQR_LIMBS = Ref(3300)
+gpu_pays(m::Int, n::Int) = m + n >= GPU_MIN_OUT_LIMBS[]
 gpu_pays_sqr(n::Int) = n >= GPU_MIN_SQR_LIMBS[]
 
 # Replaces the engine entry points of the enclosing NativeBigInt module so that
@@ -177,11 +180,11 @@ gpu_pays_sqr(n::Int) = n >= GPU_MIN_SQR_LIMBS[]
 # reference's own CPU methods stay reachable for the smaller products: they are
 # called in the world age captured before the replacement
 # (Base.invoke_in_world), so nothing of the CPU engine is copied.
-# min_limbs / min_sqr_limbs override the measured crossover (0: every product
-# on the GPU).
-function install!(mod::Module = parentmodule(@__MODULE__); min_limbs::Int = GPU_MIN_LIMBS[],
+# min_out_limbs / min_sqr_limbs override the measured crossover (0: every
+# product on the GPU).
+function install!(mod::Module = parentmodule(@__MODULE__); min_out_limbs::Int = GPU_MIN_OUT_LIMBS[],
                   min_sqr_limbs::Int = GPU_MIN_SQR_LIMBS[])
-    GPU_MIN_LIMBS[] = min_limbs
+    GPU_MIN_OUT_LIMBS[] = min_out_limbs
     GPU_MIN_SQR_LIMBS[] = min_sqr_limbs
     world = Base.get_world_counter()
     cpu_mul = getfield(mod, :mul_fpntt2!)

@@ -678,7 +678,7 @@ int nbg_batch_profile(nbg_batch* bt, void* stream, float* ms, int32_t cap) {
     CUDA_TRY(cudaEventRecord(ev[0], st));
     for (size_t i = 0; i < ls.size(); i++) {
         const Launch& L = ls[i];
-        cudaError_t e = launch_jobs(L.kind, prods, g_eng.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st, L.variant);
+        cudaError_t e = launch_jobs(L.kind, prods, g_eng.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st, L.odd);
         if (e != cudaSuccess) { rc = fail(NBG_ECUDA, "profile launch: %s", cudaGetErrorString(e)); break; }
         g_launches++;
         CUDA_TRY(cudaEventRecord(ev[i + 1], st));

@@ -811,10 +811,10 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         int mode = JM_SEGS;
         double ops = 0, bytes = 0;
     };
-    // key: (step order, kind, smem, kernel variant: VAR_* bits)
+    // key: (step order, kind, smem, odd stages present)
     std::map<std::tuple<int, int, size_t, int>, Group> groups;
-    auto group_of = [&](int order, int kind, size_t smem, bool odd = false, bool pack = false) -> Group& {
-        return groups[std::make_tuple(order, kind, smem, (odd ? VAR_ODD : 0) | (pack ? VAR_PACK : 0))];
+    auto group_of = [&](int order, int kind, size_t smem, bool odd = false) -> Group& {
+        return groups[std::make_tuple(order, kind, smem, odd ? 1 : 0)];
     };
     auto pass_odd = [](const DPlan& pl, const DPass& ps) {
         for (int st = ps.sa; st <= ps.sb; st++)
@@ -932,8 +932,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
                                 (size_t)tile_stride_doubles(ps.G * ps.C);
             const double pts = (double)ps.G * ps.C;
             const double jobs = (double)ps.ntiles * nc;  // tiles of both primes (the work, split or not)
-            Group& g = group_of(pmax - 1, keep ? JK_PWR_KEEP : split ? JK_PWR_SPLIT : JK_PWR, smem, pass_odd(pl, ps),
-                                Pn == 1);
+            Group& g = group_of(pmax - 1, keep ? JK_PWR_KEEP : split ? JK_PWR_SPLIT : JK_PWR, smem, pass_odd(pl, ps));
             emit(g, ps, split ? 2 : 1, (Pn - 1) << 8);  // split: "operand" is the prime
             g.ops += jobs * 2.0 * (nop * pass_ops(pl, ps, true) + 7.0 * pts + pass_ops(pl, ps, false));
             const double in_b = Pn == 1 ? (double)ps.ntiles * nop * pts * sum_bch / 8.0 : jobs * 2.0 * nop * 8.0 * pts;
@@ -986,7 +985,7 @@ int build_batch(Engine& E, const ProdIn* in, int64_t count, BatchBuild& bb) {
         const Group& g = kv.second;
         const int kind = std::get<1>(kv.first);
         Launch L{kind, bb.total_jobs, g.njobs, std::get<2>(kv.first)};
-        L.variant = std::get<3>(kv.first);
+        L.odd = std::get<3>(kv.first) != 0;
         bb.total_jobs += g.njobs;
         L.step = std::get<0>(kv.first);
         L.alg_ops = g.ops;
@@ -1120,7 +1119,7 @@ int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, 
         g_launches++;
     }
     for (const Launch& L : bb.launches) {
-        cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st, L.variant);
+        cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, st, L.odd);
         if (e != cudaSuccess) return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n,
                                           cudaGetErrorString(e));
         g_launches++;
@@ -1152,7 +1151,7 @@ int run_launches_branched(Engine& E, const BatchBuild& bb, char* dbase, cudaStre
                 s = side[(k - i - 1) % (size_t)nside];
                 CUDA_TRY(cudaStreamWaitEvent(s, fork, 0));
             }
-            cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, s, L.variant);
+            cudaError_t e = launch_jobs(L.kind, prods, E.d_plans, job_list(jobs + L.off), L.n, L.smem, 0, s, L.odd);
             if (e != cudaSuccess)
                 return fail(NBG_ECUDA, "launch (kind %d, %lld jobs): %s", L.kind, (long long)L.n, cudaGetErrorString(e));
             g_launches++;

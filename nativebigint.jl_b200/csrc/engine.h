@@ -111,7 +111,7 @@ struct Launch {
     int nseg = 0;
     size_t seg_off = 0, plist_off = 0;
     int step = 0;          // pipeline step: launches of one step are independent
-    int variant = VAR_ALL; // VAR_ODD: some pass holds a radix-3/5/7 stage; VAR_PACK: some product packs limbs
+    bool odd = true;       // some pass of the launch holds a radix-3/5/7 stage
     double alg_ops = 0;    // FP64 instructions of the reference schedule done by this launch
     double alg_bytes = 0;  // compulsory global bytes (operand/limb reads, tile loads and stores)
 };

@@ -249,22 +249,14 @@ __device__ __forceinline__ void bf4(double& a, double& b, double& c, double& d, 
     if (!FWD) dft4(a, b, c, d, wi, F);
 }
 
-// Offset of a unit's point k from its point 0: 2^LS elements apart on a
-// dense tile; on a padded single-column tile (one double in 16) the padding
-// adds (k 2^LS) / 16 more (see round_r16_c1).
-template <int LS, bool PADL>
-__device__ __forceinline__ constexpr int r16_off(int k) {
-    return PADL ? (k << LS) + ((k << LS) >> 4) : (k << LS);
-}
-
-template <bool FWD, int LS, int PR, bool PADL = false>
+template <bool FWD, int LS, int PR>
 __device__ __forceinline__ void r16_unit_dense(double* __restrict__ s, const double* __restrict__ twA,
                                                const double* __restrict__ twB, uint32_t stepA, uint32_t QA,
                                                uint32_t QB, double wi) {
     const Fp F = c_fp[PR];
     double v[16];
 #pragma unroll
-    for (int k = 0; k < 16; k++) v[k] = s[r16_off<LS, PADL>(k)];
+    for (int k = 0; k < 16; k++) v[k] = s[k << LS];
     if (FWD) {
 #pragma unroll
         for (int t2 = 0; t2 < 4; t2++) {
@@ -287,48 +279,7 @@ __device__ __forceinline__ void r16_unit_dense(double* __restrict__ s, const dou
         }
     }
 #pragma unroll
-    for (int k = 0; k < 16; k++) s[r16_off<LS, PADL>(k)] = v[k];
-}
-
-// Radix-16 round on padded single-column tiles (the last pass: C = 1, Qb = 1,
-// j0 = 0), any tile count (k_pwr's a/b tiles of one or both primes): unit
-// (block b, row j2 < q16 = 2^LS) holds rows 16 q16 b + j2 + k q16.  With
-// j2 < q16 <= 16 or q16 a multiple of 16, the padded offset of point k is
-// lay(first point) + r16_off<LS, true>(k): compile-time.  Used by the last
-// pass of multi-pass products (k_pwr built without the pack, PACK = false).
-template <bool FWD, int LS>
-__device__ NBG_ROUND void round_r16_c1(const Tiles& T, const DStage& A, const DStage& B) {
-    const int per = T.G >> 4;
-    const int total = per * T.ntiles;
-    const uint32_t QA = (uint32_t)A.Q, QB = (uint32_t)B.Q;
-    const uint32_t stepA = 1u << LS;
-    const double wi0 = A.rot[0][0], wi1 = A.rot[1][0];
-    const double *twA0 = A.tw[0], *twA1 = A.tw[1], *twB0 = B.tw[0], *twB1 = B.tw[1];
-    for (int u = threadIdx.x; u < total; u += blockDim.x) {
-        int tau;
-        const int r = split_unit(u, per, tau);
-        const bool p1 = T.pfix >= 0 ? T.pfix == 1 : (tau >> T.pshift) != 0;
-        const int b = r >> LS, j2 = r & ((1 << LS) - 1);
-        double* su = T.s + tau * T.stride + sp((b << (LS + 4)) + j2);
-        if (p1) r16_unit_dense<FWD, LS, 1, true>(su, twA1 + j2, twB1 + j2, stepA, QA, QB, wi1);
-        else r16_unit_dense<FWD, LS, 0, true>(su, twA0 + j2, twB0 + j2, stepA, QA, QB, wi0);
-    }
-}
-
-template <bool FWD>
-__device__ __forceinline__ void round_r16_c1_any(const Tiles& T, const DStage& A, const DStage& B) {
-    switch (__ffs((int)A.L) - 1 - 4) {  // log2(q16)
-        case 0: round_r16_c1<FWD, 0>(T, A, B); break;
-        case 1: round_r16_c1<FWD, 1>(T, A, B); break;
-        case 2: round_r16_c1<FWD, 2>(T, A, B); break;
-        case 3: round_r16_c1<FWD, 3>(T, A, B); break;
-        case 4: round_r16_c1<FWD, 4>(T, A, B); break;
-        case 5: round_r16_c1<FWD, 5>(T, A, B); break;
-        case 6: round_r16_c1<FWD, 6>(T, A, B); break;
-        case 7: round_r16_c1<FWD, 7>(T, A, B); break;
-        case 8: round_r16_c1<FWD, 8>(T, A, B); break;
-        default: round_r16<FWD, true>(T, A, B); break;
-    }
+    for (int k = 0; k < 16; k++) s[k << LS] = v[k];
 }
 
 // Tiles: prime 0 at T.s, prime 1 at T.s + T.stride (dense, row length C = 2^lc).
@@ -577,16 +528,14 @@ __device__ NBG_ROUND void fused_r8(const FuseTiles& T, const DStage& A) {
 // radix-8 or radix-2 round (those stages end a transform: the last pass).
 // ODD = false: the pass holds no radix-3/5/7 stage (every pass but the first of
 // an odd-length transform), so that code and its registers are left out.
-template <bool FWD, bool PAD = true, bool ODD = true, bool C1 = false>
+template <bool FWD, bool PAD = true, bool ODD = true>
 __device__ void run_round(const Tiles& T, const DPlan& pl, int kind, int s0) {
     __syncthreads();
     const DStage& st = pl.st[s0];
     switch (kind) {
         case RK_R16:
-            if (!PAD) round_r16_dense_any<FWD>(T, st, pl.st[s0 + 1]);
-            else if (C1 && T.lc == 0 && T.Qb == 1 && T.j0 == 0 && (st.L & (st.L - 1)) == 0)
-                round_r16_c1_any<FWD>(T, st, pl.st[s0 + 1]);
-            else round_r16<FWD, PAD>(T, st, pl.st[s0 + 1]);
+            if (PAD) round_r16<FWD, PAD>(T, st, pl.st[s0 + 1]);
+            else round_r16_dense_any<FWD>(T, st, pl.st[s0 + 1]);
             break;
         case RK_R4: round_gen<4, FWD, PAD>(T, st); break;
         case RK_R8:
@@ -604,12 +553,12 @@ __device__ void run_round(const Tiles& T, const DPlan& pl, int kind, int s0) {
     }
 }
 
-template <bool FWD, bool PAD = true, bool ODD = true, bool C1 = false>
+template <bool FWD, bool PAD = true, bool ODD = true>
 __device__ void run_pass(const Tiles& T, const DPlan& pl, const DPass& ps) {
     if (FWD) {
-        for (int r = 0; r < ps.nrounds; r++) run_round<true, PAD, ODD, C1>(T, pl, ps.rkind[r], ps.rstage[r]);
+        for (int r = 0; r < ps.nrounds; r++) run_round<true, PAD, ODD>(T, pl, ps.rkind[r], ps.rstage[r]);
     } else {
-        for (int r = ps.nrounds - 1; r >= 0; r--) run_round<false, PAD, ODD, C1>(T, pl, ps.rkind[r], ps.rstage[r]);
+        for (int r = ps.nrounds - 1; r >= 0; r--) run_round<false, PAD, ODD>(T, pl, ps.rkind[r], ps.rstage[r]);
     }
     __syncthreads();
 }
@@ -761,10 +710,8 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restr
 // Tiles: products [a0, b0, a1, b1], squares [a0, a1].
 // SPLIT: one CTA per prime (JK_PWR_SPLIT).  KEEPB: launches of products with
 // a kept operand spectrum (JK_PWR_KEEP; PF_BSAVE / PF_BSPEC), compiled apart
-// so the other launches carry none of that code.  PACK = false: every product
-// of the launch has more than one pass (nothing to pack), and the radix-16
-// rounds use the compile-time offsets of round_r16_c1.
-template <bool SPLIT, bool KEEPB, bool ODD, bool PACK>
+// so the other launches carry none of that code.
+template <bool SPLIT, bool KEEPB, bool ODD>
 __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const Job* __restrict__ jobs, int64_t njobs) {
@@ -794,7 +741,7 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
         const bool bspec = KEEPB && !sq && (P.flags & PF_BSPEC);
         const bool bsave = KEEPB && !sq && (P.flags & PF_BSAVE);
         __syncthreads();
-        if (PACK && pass == 0 && !(P.flags & PF_PRELOADED)) {
+        if (pass == 0 && !(P.flags & PF_PRELOADED)) {
             pack_tile2(a0, pf >= 0 ? a0 : a1, P.a, P.m, P.bch, P.nca, ps, base);
             if (bspec) {
                 load_tile_async(b0, P.xb[p0], ps, base);
@@ -823,7 +770,7 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
         const int lastk = ps.rkind[nr - 1];
         if (lastk == RK_R16 || lastk == RK_R8) {
             // forward rounds but the last, fused round, reverse rounds but the first
-            for (int r = 0; r < nr - 1; r++) run_round<true, true, ODD, !PACK>(TF, pl, ps.rkind[r], ps.rstage[r]);
+            for (int r = 0; r < nr - 1; r++) run_round<true, true, ODD>(TF, pl, ps.rkind[r], ps.rstage[r]);
             __syncthreads();
             FuseTiles FT;
             FT.s = smem;
@@ -844,10 +791,10 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
                 store_tile(b0, P.xb[p0], ps, base);
                 if (pf < 0) store_tile(b1, P.xb[1], ps, base);
             }
-            for (int r = nr - 2; r >= 0; r--) run_round<false, true, ODD, !PACK>(TR, pl, ps.rkind[r], ps.rstage[r]);
+            for (int r = nr - 2; r >= 0; r--) run_round<false, true, ODD>(TR, pl, ps.rkind[r], ps.rstage[r]);
             __syncthreads();
         } else {
-            run_pass<true, true, ODD, !PACK>(TF, pl, ps);
+            run_pass<true, true, ODD>(TF, pl, ps);
             if (bsave) {
                 store_tile(b0, P.xb[p0], ps, base);
                 if (pf < 0) store_tile(b1, P.xb[1], ps, base);
@@ -866,7 +813,7 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
                     a0[i] = fp_mulmod(a0[i], b0[i], F);
                 }
             }
-            run_pass<false, true, ODD, !PACK>(TR, pl, ps);
+            run_pass<false, true, ODD>(TR, pl, ps);
         }
         store_tile(a0, P.xa[p0], ps, base);
         if (pf < 0) store_tile(a1, P.xa[1], ps, base);
@@ -1412,12 +1359,9 @@ cudaError_t kernels_init(double p1, double p2) {
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const void* ks[] = {(const void*)k_fwd<3, true>, (const void*)k_fwd<4, true>, (const void*)k_fwd<3, false>,
                         (const void*)k_fwd<4, false>,
-                        (const void*)k_pwr<false, false, true, true>, (const void*)k_pwr<true, false, true, true>,
-                        (const void*)k_pwr<false, true, true, true>, (const void*)k_pwr<false, false, false, true>,
-                        (const void*)k_pwr<true, false, false, true>, (const void*)k_pwr<false, true, false, true>,
-                        (const void*)k_pwr<false, false, true, false>, (const void*)k_pwr<true, false, true, false>,
-                        (const void*)k_pwr<false, true, true, false>, (const void*)k_pwr<false, false, false, false>,
-                        (const void*)k_pwr<true, false, false, false>, (const void*)k_pwr<false, true, false, false>,
+                        (const void*)k_pwr<false, false, true>, (const void*)k_pwr<true, false, true>,
+                        (const void*)k_pwr<false, true, true>, (const void*)k_pwr<false, false, false>,
+                        (const void*)k_pwr<true, false, false>, (const void*)k_pwr<false, true, false>,
                         (const void*)k_rev<3, true>, (const void*)k_rev<4, true>, (const void*)k_rev<3, false>,
                         (const void*)k_rev<4, false>, (const void*)k_unpack,
                         (const void*)k_col_tma<3, true, true>, (const void*)k_col_tma<4, true, true>,
@@ -1446,15 +1390,14 @@ cudaError_t kernels_take_faults(unsigned int* n) {
 
 cudaError_t kernels_binary_version(int* version) {
     cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)k_pwr<false, false, false, false>);
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)k_pwr<false, false, false>);
     if (e != cudaSuccess) return e;
     *version = fa.binaryVersion;
     return cudaSuccess;
 }
 
 cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& src, int64_t njobs,
-                        size_t smem, int grid_cap, cudaStream_t st, int variant) {
-    const bool odd = (variant & VAR_ODD) != 0, pack = (variant & VAR_PACK) != 0;
+                        size_t smem, int grid_cap, cudaStream_t st, bool odd) {
     // the kernels read an explicit job list (batches expand theirs on the device first)
     if (src.mode != JM_LIST) return cudaErrorInvalidValue;
     const Job* jobs = src.list;
@@ -1489,20 +1432,9 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
             if (c4t && !odd) NBG_ODD(k_col_tma, 4, false);
             else NBG_ODD(k_col_tma, 3, false);
             break;
-#define NBG_PWR(SPLIT, KEEPB)                                                                        \
-    do {                                                                                             \
-        if (odd) {                                                                                   \
-            if (pack) k_pwr<SPLIT, KEEPB, true, true><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);   \
-            else k_pwr<SPLIT, KEEPB, true, false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);       \
-        } else {                                                                                     \
-            if (pack) k_pwr<SPLIT, KEEPB, false, true><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);  \
-            else k_pwr<SPLIT, KEEPB, false, false><<<grid, 256, smem, st>>>(prods, plans, jobs, njobs);      \
-        }                                                                                            \
-    } while (0)
-        case JK_PWR: NBG_PWR(false, false); break;
-        case JK_PWR_SPLIT: NBG_PWR(true, false); break;
-        case JK_PWR_KEEP: NBG_PWR(false, true); break;
-#undef NBG_PWR
+        case JK_PWR: NBG_ODD(k_pwr, false, false); break;
+        case JK_PWR_SPLIT: NBG_ODD(k_pwr, true, false); break;
+        case JK_PWR_KEEP: NBG_ODD(k_pwr, false, true); break;
         case JK_REV:
             if (c4) NBG_ODD(k_rev, 4);
             else NBG_ODD(k_rev, 3);

@@ -23,11 +23,9 @@ inline JobSrc job_list(const Job* l) {
 }
 
 // One work-queue launch of `kind` (JobKind) over jobs 0..njobs-1 of `jobs`.
-// variant (VAR_* bits) without VAR_ODD: no pass of the launch holds a
-// radix-3/5/7 stage; without VAR_PACK: no product packs limbs in it (leaner
-// kernel builds).
+// odd = false: no pass of the launch holds a radix-3/5/7 stage (a leaner kernel build).
 cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& jobs, int64_t njobs,
-                        size_t smem, int grid_cap, cudaStream_t st, int variant = VAR_ALL);
+                        size_t smem, int grid_cap, cudaStream_t st, bool odd = true);
 
 // Writes a batch's explicit job list from its compact description: out[g] for
 // every g < total, entry e covering [e.begin, e.begin + e.n).

@@ -186,12 +186,6 @@ enum JobKind : int32_t {
     JK_REV_TMA = 9,  // JK_REV with tiles staged by TMA
 };
 
-// Kernel build variants of a launch (bit mask): some pass holds a radix-3/5/7
-// stage; some product packs limbs in the launch (a one-pass product's last pass).
-constexpr int VAR_ODD = 1;
-constexpr int VAR_PACK = 2;
-constexpr int VAR_ALL = VAR_ODD | VAR_PACK;
-
 constexpr int UNPACK_TL = 1024;  // output limbs per unpack tile
 // Dynamic shared memory of one unpack tile for chunk width b: (lo, hi) pairs of
 // the coefficients that start in bits [64 (w0 - 4), 64 (w0 + UNPACK_TL)).

@@ -1046,16 +1046,17 @@ __device__ __forceinline__ void window_add(uint64_t& W0, uint64_t& W1, uint64_t&
 // in bits [64 wt, 64 (wt + 4)); d = b i - 64 wt), streamed through a 3-word
 // window; the part above the range comes back as the spill (s0, s1), limbs
 // wt + 4 and wt + 5.  OWN = false keeps only the spill.
+// (k, kend: coefficient indices relative to the tile's first, ibase; 32-bit)
 template <bool OWN>
-__device__ __forceinline__ void range_limbs(const ulonglong2* __restrict__ cs, int64_t ibase, int64_t i, int64_t iend,
-                                            uint32_t d, uint32_t b, uint64_t* own, uint64_t& s0, uint64_t& s1) {
+__device__ __forceinline__ void range_limbs(const ulonglong2* __restrict__ cs, int k, int kend, uint32_t d,
+                                            uint32_t b, uint64_t* own, uint64_t& s0, uint64_t& s1) {
     uint64_t W0 = 0, W1 = 0, W2 = 0;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        while (i <= iend && d < 64) {
-            const ulonglong2 c = cs[i - ibase];
+        while (k <= kend && d < 64) {
+            const ulonglong2 c = cs[k];
             window_add(W0, W1, W2, c.x, c.y, d);
-            i++;
+            k++;
             d += b;
         }
         if (OWN) own[q] = W0;
@@ -1131,7 +1132,8 @@ __global__ void __launch_bounds__(UNPACK_THREADS, 4) k_unpack(const DProd* __res
         {
             const int64_t i0 = div_b(64 * wt + b - 1, b, rb);
             const int64_t i1 = min(div_b(64 * (wt + 4) - 1, b, rb), ihi);
-            range_limbs<true>(ucs, ilo, i0, i1, (uint32_t)(b * i0 - 64 * wt), (uint32_t)b, own, s0, s1);
+            range_limbs<true>(ucs, (int)(i0 - ilo), (int)(i1 - ilo), (uint32_t)(b * i0 - 64 * wt), (uint32_t)b, own,
+                              s0, s1);
         }
         spill[t + 1][0] = s0;
         spill[t + 1][1] = s1;
@@ -1140,7 +1142,8 @@ __global__ void __launch_bounds__(UNPACK_THREADS, 4) k_unpack(const DProd* __res
             if (w0 > 0) {  // the spill of the range [w0 - 4, w0) into limbs w0, w0 + 1
                 const int64_t i0 = ilo;
                 const int64_t i1 = min(div_b(64 * w0 - 1, b, rb), ihi);
-                range_limbs<false>(ucs, ilo, i0, i1, (uint32_t)(b * i0 - 64 * wlo), (uint32_t)b, nullptr, p0, p1);
+                range_limbs<false>(ucs, (int)(i0 - ilo), (int)(i1 - ilo), (uint32_t)(b * i0 - 64 * wlo), (uint32_t)b,
+                                   nullptr, p0, p1);
             }
             spill[0][0] = p0;
             spill[0][1] = p1;

@@ -9,7 +9,9 @@
 //             the same shared-memory block; packs on load for one-pass products
 //   k_rev     reverse pass of one tile (fp_ntt_rev!, :727-733)
 //   k_unpack  Garner CRT (fp_unpack_coeff, :806-816) and limb assembly of a
-//             1024-limb output tile with a block-wide carry-lookahead scan
+//             1024-limb output tile with a block-wide carry-lookahead scan;
+//             persistent CTAs stage the next tile's residues by bulk copy
+//             while assembling the current one
 //   k_carry   cross-tile carry scan and fix-up, one CTA per product
 //   k_twiddle expands exact minimal-balanced twiddle tables from two small
 //             power tables (twiddle values are unique residues, so any exact
@@ -904,6 +906,13 @@ __device__ __forceinline__ void load3(void* dst, const void* map, int x, int y, 
         ::"r"(saddr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(saddr(bar))
         : "memory");
 }
+// untiled bulk copy of `bytes` (a multiple of 16) from 16-byte aligned global
+// memory of this GPU into 16-byte aligned shared memory, completing on bar
+__device__ __forceinline__ void load1(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(saddr(dst)), "l"(src), "r"(bytes), "r"(saddr(bar))
+                 : "memory");
+}
 __device__ __forceinline__ void store3(const void* map, int x, int y, int z, const void* src) {
     asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];"
                  ::"l"(map), "r"(x), "r"(y), "r"(z), "r"(saddr(src))
@@ -1013,11 +1022,6 @@ __device__ __forceinline__ void garner_xy(double x1v, double x2v, const DPlan& p
     hi = phi + (lo < plo ? 1ULL : 0ULL);
 }
 
-__device__ __forceinline__ void garner(const double* __restrict__ x1, const double* __restrict__ x2, int64_t idx,
-                                       const DPlan& pl, uint64_t& lo, uint64_t& hi) {
-    garner_xy(__ldg(x1 + idx), __ldg(x2 + idx), pl, lo, hi);
-}
-
 constexpr int UNPACK_THREADS = 256;
 constexpr int LIMBS_PER_THREAD = UNPACK_TL / UNPACK_THREADS;
 static_assert(LIMBS_PER_THREAD == 4, "the limb window below is written for 4 limbs per thread");
@@ -1042,20 +1046,20 @@ __device__ __forceinline__ void window_add(uint64_t& W0, uint64_t& W1, uint64_t&
         : "l"(a0), "l"(a1), "l"(a2));
 }
 
-// Limbs [wt, wt + 4) of the sum of the coefficients i..iend (those that start
-// in bits [64 wt, 64 (wt + 4)); d = b i - 64 wt), streamed through a 3-word
-// window; the part above the range comes back as the spill (s0, s1), limbs
-// wt + 4 and wt + 5.  OWN = false keeps only the spill.
-// (k, kend: coefficient indices relative to the tile's first, ibase; 32-bit)
+// Limbs [wt, wt + 4) of the sum of the tile's coefficients k..kend (those that
+// start in bits [64 wt, 64 (wt + 4)); d = b i - 64 wt), streamed through a
+// 3-word window; the part above the range comes back as the spill (s0, s1),
+// limbs wt + 4 and wt + 5.  OWN = false keeps only the spill.  Coefficient k's
+// 128-bit value is (u1[top1 - k], u2[top2 - k]).
 template <bool OWN>
-__device__ __forceinline__ void range_limbs(const ulonglong2* __restrict__ cs, int k, int kend, uint32_t d,
-                                            uint32_t b, uint64_t* own, uint64_t& s0, uint64_t& s1) {
+__device__ __forceinline__ void range_limbs(const uint64_t* __restrict__ u1, const uint64_t* __restrict__ u2,
+                                            int top1, int top2, int k, int kend, uint32_t d, uint32_t b,
+                                            uint64_t* own, uint64_t& s0, uint64_t& s1) {
     uint64_t W0 = 0, W1 = 0, W2 = 0;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         while (k <= kend && d < 64) {
-            const ulonglong2 c = cs[k];
-            window_add(W0, W1, W2, c.x, c.y, d);
+            window_add(W0, W1, W2, u1[top1 - k], u2[top2 - k], d);
             k++;
             d += b;
         }
@@ -1078,76 +1082,163 @@ __device__ __forceinline__ int64_t div_b(int64_t x, int b, double rb) {
     return q;
 }
 
-__global__ void __launch_bounds__(UNPACK_THREADS, 4) k_unpack(const DProd* __restrict__ prods,
+// One unpack tile: output limbs [w0, w1) and the coefficients ilo..ihi that
+// start in bits [64 wlo, 64 w1), wlo = w0 - 4 (the 4-limb range below the tile
+// spills into limbs w0 and w0 + 1).
+struct UTile {
+    int64_t w0, w1, wlo, ilo, ihi, ncoef;
+};
+
+__device__ __forceinline__ UTile unpack_tile(const DProd& P, int64_t tile) {
+    const int b = P.bch;
+    const double rb = 1.0 / (double)b;
+    UTile g;
+    g.w0 = tile * UNPACK_TL;
+    g.w1 = min(g.w0 + (int64_t)UNPACK_TL, P.rn);
+    g.wlo = g.w0 >= 4 ? g.w0 - 4 : 0;
+    g.ilo = div_b(64 * g.wlo + b - 1, b, rb);
+    g.ihi = min(div_b(64 * g.w1 - 1, b, rb), P.nconv - 1);
+    g.ncoef = g.ihi >= g.ilo ? g.ihi - g.ilo + 1 : 0;
+    return g;
+}
+
+// Coefficient i > 0 has its residues at x[N - i], so the tile's residues
+// (i = 0 apart: x[0], read directly) are the contiguous run x[N - ihi ..
+// N - max(ilo, 1)], descending in i.  One untiled bulk copy per prime stages
+// the run, widened to 16-byte boundaries (a 16-byte block holding a valid
+// double lies inside the same allocation); the run starts `lead` (0 or 1)
+// doubles into the stage.
+__device__ __forceinline__ int stage_lead(const double* x, int64_t N, const UTile& g) {
+    return (int)((reinterpret_cast<uintptr_t>(x + (N - g.ihi)) >> 3) & 1);
+}
+
+__device__ __forceinline__ void unpack_issue(const DProd& P, int64_t N, const UTile& g, double* st1, double* st2,
+                                             uint64_t* bar) {
+    const int64_t cnt = g.ncoef - (g.ilo == 0 ? 1 : 0);
+    if (cnt <= 0) {
+        tma::bar_expect(bar, 0);  // nothing to stage: the phase completes with this arrival
+        return;
+    }
+    uintptr_t src[2];
+    uint32_t bytes[2];
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(P.xa[f] + (N - g.ihi));
+        src[f] = a & ~(uintptr_t)15;
+        bytes[f] = (uint32_t)(((a + 8 * (uintptr_t)cnt + 15) & ~(uintptr_t)15) - src[f]);
+    }
+    tma::bar_expect(bar, bytes[0] + bytes[1]);
+    tma::load1(st1, reinterpret_cast<const void*>(src[0]), bytes[0], bar);
+    tma::load1(st2, reinterpret_cast<const void*>(src[1]), bytes[1], bar);
+}
+
+// Persistent: CTA c assembles tiles c, c + G, c + 2G, ... (G = gridDim.x); the
+// next tile's residues are in flight (bulk copy into the other stage) while
+// this one is assembled.  Dynamic shared memory: [2 mbarriers | 112 B |
+// stage 0 (prime 1, prime 2) | stage 1], each prime's part `cap` doubles.
+__global__ void __launch_bounds__(UNPACK_THREADS, 3) k_unpack(const DProd* __restrict__ prods,
                                                               const DPlan* __restrict__ plans,
                                                               const Job* __restrict__ jobs, int64_t njobs) {
-    extern __shared__ ulonglong2 ucs[];
+    extern __shared__ __align__(128) double dsm[];
     __shared__ uint32_t wagg[UNPACK_THREADS / 32];
     __shared__ uint64_t spill[UNPACK_THREADS + 1][2];
-    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm);
+    uint32_t dsz;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dsz));
+    const int cap = (int)((dsz - 128) / 32);
+    double* const stg = dsm + 16;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        tma::bar_init(bar);
+        tma::bar_init(bar + 1);
+    }
+    __syncthreads();
+    int j = 0;
+    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x, j++) {
+        const int s = j & 1;
+        double* const st1 = stg + (size_t)s * 2 * cap;
+        double* const st2 = st1 + cap;
         const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int b = P.bch;
         const int64_t N = pl.N;
-        const int64_t w0 = jb.tile * UNPACK_TL;
-        const int64_t w1 = min(w0 + (int64_t)UNPACK_TL, P.rn);
-        // coefficients that start in bits [64 (w0 - 4), 64 w1): the tile's own and
-        // those of the 4-limb range below it, whose spill reaches limb w0
-        const int64_t wlo = w0 >= 4 ? w0 - 4 : 0;
-        const double rb = 1.0 / (double)b;
-        const int64_t ilo = div_b(64 * wlo + b - 1, b, rb);
-        int64_t ihi = div_b(64 * w1 - 1, b, rb);
-        if (ihi > P.nconv - 1) ihi = P.nconv - 1;
-        const int64_t ncoef = ihi >= ilo ? ihi - ilo + 1 : 0;
-        __syncthreads();
-        // Garner, four coefficients per thread at a time: their eight loads are
-        // in flight together before the arithmetic
-        const double* __restrict__ x1 = P.xa[0];
-        const double* __restrict__ x2 = P.xa[1];
-        for (int64_t k0 = threadIdx.x; k0 < ncoef; k0 += 4 * (int64_t)blockDim.x) {
-            double a1[4], a2[4];
+        const UTile g = unpack_tile(P, jb.tile);
+        const int64_t jn = ji + gridDim.x;
+        if (t == 0) {
+            if (j == 0) unpack_issue(P, N, g, st1, st2, bar + s);
+            if (jn < njobs) {  // stage s ^ 1 was last read before the previous tile's spill exchange
+                const Job jx = jobs[jn];
+                const DProd& Px = prods[jx.prod];
+                double* const nx = stg + (size_t)(s ^ 1) * 2 * cap;
+                unpack_issue(Px, plans[Px.plan].N, unpack_tile(Px, jx.tile), nx, nx + cap, bar + (s ^ 1));
+            }
+        }
+        if (!tma::bar_wait(bar + s, (uint32_t)(j >> 1) & 1u)) {
+            // gave up (counted): let the copy in flight into the other stage land first
+            if (jn < njobs) tma::bar_wait(bar + (s ^ 1), (uint32_t)((j + 1) >> 1) & 1u);
+            return;
+        }
+        const int nc = (int)g.ncoef;
+        const int top1 = stage_lead(P.xa[0], N, g) + nc - 1;
+        const int top2 = stage_lead(P.xa[1], N, g) + nc - 1;
+        uint64_t* const u1 = reinterpret_cast<uint64_t*>(st1);
+        uint64_t* const u2 = reinterpret_cast<uint64_t*>(st2);
+        // Garner in place: coefficient k's two residues become its (lo, hi)
+        for (int k0 = t; k0 < nc; k0 += 8 * UNPACK_THREADS) {
+            double a1[8], a2[8];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int64_t k = k0 + q * (int64_t)blockDim.x;
-                const int64_t i = ilo + k;
-                const int64_t idx = k < ncoef ? (i == 0 ? 0 : N - i) : 0;
-                a1[q] = __ldg(x1 + idx);
-                a2[q] = __ldg(x2 + idx);
+            for (int q = 0; q < 8; q++) {
+                const int k = k0 + q * UNPACK_THREADS;
+                a1[q] = 0.0;
+                a2[q] = 0.0;
+                if (k < nc) {
+                    if (k == 0 && g.ilo == 0) {
+                        a1[q] = __ldg(P.xa[0]);
+                        a2[q] = __ldg(P.xa[1]);
+                    } else {
+                        a1[q] = st1[top1 - k];
+                        a2[q] = st2[top2 - k];
+                    }
+                }
             }
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int64_t k = k0 + q * (int64_t)blockDim.x;
-                if (k < ncoef) {
+            for (int q = 0; q < 8; q++) {
+                const int k = k0 + q * UNPACK_THREADS;
+                if (k < nc) {
                     uint64_t lo, hi;
                     garner_xy(a1[q], a2[q], pl, lo, hi);
-                    ucs[k] = make_ulonglong2(lo, hi);
+                    u1[top1 - k] = lo;
+                    u2[top2 - k] = hi;
                 }
             }
         }
         __syncthreads();
-        const int t = threadIdx.x;
+        const int64_t w0 = g.w0, w1 = g.w1, ilo = g.ilo, ihi = g.ihi;
+        const double rb = 1.0 / (double)b;
         const int64_t wt = w0 + 4 * (int64_t)t;
         uint64_t own[4], s0, s1;
         {
             const int64_t i0 = div_b(64 * wt + b - 1, b, rb);
             const int64_t i1 = min(div_b(64 * (wt + 4) - 1, b, rb), ihi);
-            range_limbs<true>(ucs, (int)(i0 - ilo), (int)(i1 - ilo), (uint32_t)(b * i0 - 64 * wt), (uint32_t)b, own,
-                              s0, s1);
+            range_limbs<true>(u1, u2, top1, top2, (int)(i0 - ilo), (int)(i1 - ilo), (uint32_t)(b * i0 - 64 * wt),
+                              (uint32_t)b, own, s0, s1);
         }
         spill[t + 1][0] = s0;
         spill[t + 1][1] = s1;
         if (t == 0) {
             uint64_t p0 = 0, p1 = 0;
             if (w0 > 0) {  // the spill of the range [w0 - 4, w0) into limbs w0, w0 + 1
-                const int64_t i0 = ilo;
                 const int64_t i1 = min(div_b(64 * w0 - 1, b, rb), ihi);
-                range_limbs<false>(ucs, (int)(i0 - ilo), (int)(i1 - ilo), (uint32_t)(b * i0 - 64 * wlo), (uint32_t)b,
-                                   nullptr, p0, p1);
+                range_limbs<false>(u1, u2, top1, top2, 0, (int)(i1 - ilo), (uint32_t)(b * ilo - 64 * g.wlo),
+                                   (uint32_t)b, nullptr, p0, p1);
             }
             spill[0][0] = p0;
             spill[0][1] = p1;
         }
+        // this stage's generic-proxy accesses come before the bulk copy that
+        // refills it (issued after the barrier below)
+        tma::fence_async();
         __syncthreads();
         // own + the spill from below: a carry (0 or 1) out of the 4 limbs, then
         // generate / propagate across threads
@@ -1337,6 +1428,7 @@ __global__ void k_twiddle(double* __restrict__ out, int m, int64_t Q, int64_t st
 // Written once per kernels_init with its final value, so a concurrent reader
 // never sees a partial result.
 static std::atomic<int> g_smem_optin{0};
+static std::atomic<int> g_num_sms{148};
 
 cudaError_t kernels_init(double p1, double p2) {
     Fp h[2] = {{p1, 1.0 / p1}, {p2, 1.0 / p2}};
@@ -1378,6 +1470,10 @@ cudaError_t kernels_init(double p1, double p2) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
         if (e != cudaSuccess) return e;
     }
+    int nsm = 0;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    g_num_sms.store(nsm);
     g_smem_optin.store(optin - 8192);  // headroom for the largest static allocation (k_unpack, 4.1 KB)
     return cudaSuccess;
 }
@@ -1442,7 +1538,15 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
             if (c4) NBG_ODD(k_rev, 4);
             else NBG_ODD(k_rev, 3);
             break;
-        case JK_UNPACK: k_unpack<<<grid, UNPACK_THREADS, smem, st>>>(prods, plans, jobs, njobs); break;
+        case JK_UNPACK: {
+            // persistent: as many CTAs as fit on the GPU at once, each streaming its tiles
+            int nb = 0;
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_unpack, UNPACK_THREADS, smem);
+            if (e != cudaSuccess) return e;
+            const unsigned g = (unsigned)std::min<int64_t>(grid, (int64_t)std::max(nb, 1) * g_num_sms.load());
+            k_unpack<<<g, UNPACK_THREADS, smem, st>>>(prods, plans, jobs, njobs);
+            break;
+        }
         case JK_CARRY: k_carry<<<grid, 256, 0, st>>>(prods, jobs, njobs); break;
         case JK_CARRYFIX: {
             // one warp per tile (most tiles are left at once)

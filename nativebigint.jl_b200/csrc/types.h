@@ -187,12 +187,18 @@ enum JobKind : int32_t {
 };
 
 constexpr int UNPACK_TL = 1024;  // output limbs per unpack tile
-// Dynamic shared memory of one unpack tile for chunk width b: (lo, hi) pairs of
-// the coefficients that start in bits [64 (w0 - 4), 64 (w0 + UNPACK_TL)).
-NBG_HD inline size_t unpack_smem_bytes(int b) {
+// Residues staged per prime for one unpack tile of chunk width b: the
+// coefficients that start in bits [64 (w0 - 4), 64 (w0 + UNPACK_TL)), plus one
+// double at each end for the 16-byte alignment of the bulk copy (kept even).
+NBG_HD inline int64_t unpack_stage_doubles(int b) {
     const int64_t ncoef = (64 * (int64_t)(UNPACK_TL + 4)) / b + 2;
-    return 16 * (size_t)ncoef;
+    return (ncoef + 3) & ~(int64_t)1;
 }
+// Dynamic shared memory of the unpack kernel: 128 bytes of mbarriers, then two
+// stages (the tile being assembled and the next one in flight) of both primes'
+// staged residues.  For the chunk widths of transforms up to 2^32 points
+// (b >= 33) this is at most 64 KB.
+NBG_HD inline size_t unpack_smem_bytes(int b) { return 128 + 2 * 2 * 8 * (size_t)unpack_stage_doubles(b); }
 constexpr int PASS_THREADS = 256;
 
 // Shared-memory tiles are padded by one double every 16 so that strided

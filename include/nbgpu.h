@@ -279,7 +279,11 @@ int nbg_plan_info(int64_t N, int32_t *nst, int32_t *npass, int32_t *stage_m, int
 int nbg_plan_layout(int64_t N, int32_t sqr, int64_t *stages, int32_t *nst, int64_t *passes, int32_t *npass,
                     int32_t *rounds, int32_t cap);
 /* Tuning knobs (JSON object, keys: full_max_mul, full_max_sqr, last_max,
- * last_max_sqr, early_gmax, tile_target, cmax, and "overrides": a list of
+ * last_max_sqr, early_gmax, tile_target, cmax, tma (1: column tiles staged by
+ * TMA), queue (0: an nbg_batch replays one launch per pipeline step and
+ * kernel kind; k in 1..64: one persistent work-queue launch whose CTAs claim
+ * k jobs at a time and wait per product for the previous step), and
+ * "overrides": a list of
  * {"N", "sqr", "pass_ends": [last stage of each pass], "tile_target", "cmax"}
  * giving an explicit pass split per transform class).  Changing them drops
  * cached plans. */

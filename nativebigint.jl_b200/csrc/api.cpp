@@ -574,6 +574,7 @@ struct nbg_batch {
     char* dmem = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    QueueRun q;  // tuning "queue" > 0: the graph is one persistent work-queue launch
 };
 
 int nbg_batch_create(const nbg_desc* descs, int64_t count, nbg_batch** out) {
@@ -604,6 +605,8 @@ int nbg_batch_create(const nbg_desc* descs, int64_t count, nbg_batch** out) {
         return fail(NBG_ENOMEM, "batch workspace of %zu bytes unavailable", want);
     }
     rc = upload_batch(E, bt->bb, bt->dmem, E.stream);
+    const bool queue = E.tun.queue > 0;
+    if (!rc && queue) rc = queue_prepare(E, bt->bb, bt->dmem, bt->q, E.stream);
     if (!rc && cudaStreamSynchronize(E.stream) != cudaSuccess) rc = fail(NBG_ECUDA, "batch upload failed");
     if (!rc) {
         cudaStream_t cs;
@@ -617,8 +620,10 @@ int nbg_batch_create(const nbg_desc* descs, int64_t count, nbg_batch** out) {
                 rc = fail(NBG_ECUDA, "begin capture failed");
             } else {
                 int64_t before = g_launches.load();
-                // a step's launches (one per shared-memory size) become parallel graph branches
-                int rl = run_launches_branched(E, bt->bb, bt->dmem, cs, side, NSIDE);
+                // a step's launches (one per shared-memory size) become parallel
+                // graph branches, or the whole batch is one work-queue launch
+                int rl = queue ? queue_run(E, bt->bb, bt->dmem, bt->q, cs)
+                               : run_launches_branched(E, bt->bb, bt->dmem, cs, side, NSIDE);
                 g_launches.store(before);  // captured, not issued
                 cudaError_t ec = cudaStreamEndCapture(cs, &bt->graph);
                 if (rl) rc = rl;
@@ -634,6 +639,7 @@ int nbg_batch_create(const nbg_desc* descs, int64_t count, nbg_batch** out) {
         if (bt->exec) cudaGraphExecDestroy(bt->exec);
         if (bt->graph) cudaGraphDestroy(bt->graph);
         cudaFree(bt->dmem);
+        queue_free(bt->q);
         delete bt;
         return rc;
     }
@@ -645,7 +651,7 @@ int nbg_batch_run(nbg_batch* bt, void* stream) {
     if (!bt) return fail(NBG_EINVAL, "null batch");
     API_LOCK_DEV();
     CUDA_TRY(cudaGraphLaunch(bt->exec, as_stream(stream)));
-    g_launches += (int64_t)bt->bb.launches.size();
+    g_launches += bt->q.d ? 2 : (int64_t)bt->bb.launches.size();
     return NBG_OK;
 }
 
@@ -695,6 +701,7 @@ int nbg_batch_destroy(nbg_batch* bt) {
     if (bt->exec) cudaGraphExecDestroy(bt->exec);
     if (bt->graph) cudaGraphDestroy(bt->graph);
     if (bt->dmem) cudaFree(bt->dmem);
+    queue_free(bt->q);
     delete bt;
     return NBG_OK;
 }

@@ -205,8 +205,9 @@ std::string Tuning::to_json() const {
     char buf[512];
     snprintf(buf, sizeof buf,
              "{\"full_max_mul\": %d, \"full_max_sqr\": %d, \"last_max\": %d, \"last_max_sqr\": %d, "
-             "\"early_gmax\": %d, \"tile_target\": %d, \"cmax\": %d, \"tma\": %d, \"overrides\": [",
-             full_max_mul, full_max_sqr, last_max, last_max_sqr, early_gmax, tile_target, cmax, tma);
+             "\"early_gmax\": %d, \"tile_target\": %d, \"cmax\": %d, \"tma\": %d, \"queue\": %d, "
+             "\"overrides\": [",
+             full_max_mul, full_max_sqr, last_max, last_max_sqr, early_gmax, tile_target, cmax, tma, queue);
     std::string out = buf;
     bool first = true;
     for (const auto& kv : overrides) {
@@ -275,13 +276,14 @@ int Tuning::from_json(const char* js) {
     json_int(head.c_str(), "tile_target", &t.tile_target);
     json_int(head.c_str(), "cmax", &t.cmax);
     json_int(head.c_str(), "tma", &t.tma);
+    json_int(head.c_str(), "queue", &t.queue);
     auto pow2 = [](int v) { return v >= 1 && (v & (v - 1)) == 0; };
     // shared memory bounds: a product's last pass holds 4 tiles (a, b per
     // prime), a square's 2; column passes hold 2 tiles of <= tile_target or G.
     if (!pow2(t.cmax) || t.last_max < 4 || t.last_max_sqr < 4 || t.early_gmax < 2 || t.tile_target < 1 ||
         t.full_max_mul < 4 || t.full_max_sqr < 4 || t.full_max_mul > 4096 || t.full_max_sqr > 8192 ||
         t.last_max > 4096 || t.last_max_sqr > 8192 || t.early_gmax > 1024 || t.tile_target > 8192 ||
-        (t.tma != 0 && t.tma != 1))
+        (t.tma != 0 && t.tma != 1) || t.queue < 0 || t.queue > 64)
         return fail(NBG_EINVAL, "tuning out of range");
     if (ov) {
         t.overrides.clear();
@@ -1170,6 +1172,74 @@ int run_launches_branched(Engine& E, const BatchBuild& bb, char* dbase, cudaStre
         i = j;
     }
     return NBG_OK;
+}
+
+int queue_prepare(Engine& E, const BatchBuild& bb, char* dbase, QueueRun& q, cudaStream_t st) {
+    queue_free(q);
+    std::vector<QLaunch> tab;
+    int64_t total = 0;
+    size_t smem = 0;
+    for (const Launch& L : bb.launches) {
+        if (L.kind == JK_CARRYFIX) continue;  // the carry job fixes its own flagged tiles
+        QLaunch e{};
+        e.qstart = total;
+        e.off = L.off;
+        e.kind = L.kind;
+        e.odd = L.odd ? 1 : 0;
+        tab.push_back(e);
+        total += L.n;
+        // k_queue's region starts 128 bytes in: column TMA sizes include that
+        // header already, the unpack needs one of its two stages
+        size_t need = L.smem + 128;
+        if (L.kind == JK_FWD_TMA || L.kind == JK_REV_TMA) need = L.smem;
+        else if (L.kind == JK_UNPACK) need = 128 + (L.smem - 128) / 2;
+        else if (L.kind == JK_CARRY) need = 128;
+        smem = std::max(smem, need);
+    }
+    QLaunch end{};
+    end.qstart = total;
+    end.kind = -1;
+    tab.push_back(end);
+    if ((int)smem > E.smem_optin) return fail(NBG_EINVAL, "queue: %zu bytes of shared memory per CTA", smem);
+    const size_t nprod = bb.prods.size();
+    const size_t cnt = sizeof(uint32_t) * nprod * (size_t)QSTEPS;
+    q.off_done = align_up(sizeof(QState), 256);
+    q.zero_bytes = q.off_done + cnt;
+    q.off_need = align_up(q.zero_bytes, 256);
+    q.off_ql = align_up(q.off_need + cnt, 256);
+    q.bytes = q.off_ql + sizeof(QLaunch) * tab.size();
+    if (cudaMalloc(&q.d, q.bytes) != cudaSuccess) {
+        cudaGetLastError();
+        q.d = nullptr;
+        return fail(NBG_ENOMEM, "queue state of %zu bytes unavailable", q.bytes);
+    }
+    q.nl = (int)tab.size() - 1;
+    q.total = total;
+    q.smem = smem;
+    q.chunk = std::max(1, E.tun.queue);
+    CUDA_TRY(queue_grid(smem, &q.grid));
+    CUDA_TRY(cudaMemcpyAsync(q.d + q.off_ql, tab.data(), sizeof(QLaunch) * tab.size(), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(q.d + q.off_need, 0, cnt, st));
+    CUDA_TRY(expand_jobs(bb, dbase, st));
+    CUDA_TRY(launch_qcount((const DProd*)(dbase + bb.off_prods), (const Job*)(dbase + bb.off_joblist),
+                           (const QLaunch*)(q.d + q.off_ql), q.nl, total, (uint32_t*)(q.d + q.off_need), st));
+    return NBG_OK;
+}
+
+int queue_run(Engine& E, const BatchBuild& bb, char* dbase, const QueueRun& q, cudaStream_t st) {
+    if (!q.d) return fail(NBG_EINVAL, "queue not prepared");
+    CUDA_TRY(cudaMemsetAsync(q.d, 0, q.zero_bytes, st));
+    CUDA_TRY(expand_jobs(bb, dbase, st));
+    CUDA_TRY(launch_queue((const DProd*)(dbase + bb.off_prods), E.d_plans, (const Job*)(dbase + bb.off_joblist),
+                          (const QLaunch*)(q.d + q.off_ql), q.nl, (QState*)q.d, (uint32_t*)(q.d + q.off_done),
+                          (const uint32_t*)(q.d + q.off_need), q.smem, q.grid, q.chunk, st));
+    g_launches += 2;
+    return NBG_OK;
+}
+
+void queue_free(QueueRun& q) {
+    if (q.d) cudaFree(q.d);
+    q = QueueRun{};
 }
 
 }  // namespace nbg

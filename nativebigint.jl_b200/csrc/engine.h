@@ -39,6 +39,8 @@ struct Tuning {
     int tile_target = 4096;   // target doubles per column-pass tile (>= 16 G: TMA-eligible columns)
     int cmax = 128;           // most adjacent columns per column-pass tile
     int tma = 1;              // stage column tiles of at least 16 columns by TMA (0: cp.async for all)
+    int queue = 0;            // > 0: reusable batches run as one persistent work-queue launch (k_queue)
+                              // whose CTAs claim this many consecutive jobs at a time (at most 64)
     std::map<int64_t, SplitOverride> overrides;  // key: N * 2 + square
     std::string to_json() const;
     int from_json(const char* js);
@@ -160,7 +162,27 @@ cudaError_t expand_jobs(const BatchBuild& bb, char* dbase, cudaStream_t st);
 JobSrc launch_src(const BatchBuild& bb, const Launch& L, const char* dbase);
 // expand = false reuses the job list a previous run wrote (same region).
 int run_launches(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, bool expand = true);
-// Same, with the independent launches of each step forked onto `side`
+// Work-queue execution of a batch: one persistent launch (k_queue) walks the
+// batch's jobs in pipeline-step order.  d: [QState | done | need | table],
+// the first zero_bytes cleared before every run.
+struct QueueRun {
+    char* d = nullptr;
+    size_t bytes = 0, zero_bytes = 0;
+    size_t off_done = 0, off_need = 0, off_ql = 0;
+    int nl = 0;
+    int64_t total = 0;
+    size_t smem = 0;
+    int grid = 0;
+    int chunk = 1;  // consecutive jobs per claim
+};
+// Allocates and fills q for a bound, uploaded batch (expands its job list and
+// counts each product's jobs per step); NBG_EINVAL when a tile set and an
+// unpack stage do not fit one CTA's shared memory.
+int queue_prepare(Engine& E, const BatchBuild& bb, char* dbase, QueueRun& q, cudaStream_t st);
+// One run: clears the queue state, expands the job list, launches k_queue.
+int queue_run(Engine& E, const BatchBuild& bb, char* dbase, const QueueRun& q, cudaStream_t st);
+void queue_free(QueueRun& q);
+// run_launches with the independent launches of each step forked onto `side`
 // streams (used while capturing a CUDA graph, where they become parallel branches).
 int run_launches_branched(Engine& E, const BatchBuild& bb, char* dbase, cudaStream_t st, cudaStream_t* side,
                           int nside);

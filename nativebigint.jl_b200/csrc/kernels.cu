@@ -13,6 +13,10 @@
 //             persistent CTAs stage the next tile's residues by bulk copy
 //             while assembling the current one
 //   k_carry   cross-tile carry scan and fix-up, one CTA per product
+//   k_queue   a whole batch in one persistent launch: CTAs claim jobs from a
+//             queue in pipeline-step order and wait, per product, for the
+//             previous step's jobs (the per-kind kernels above run the same
+//             job functions)
 //   k_twiddle expands exact minimal-balanced twiddle tables from two small
 //             power tables (twiddle values are unique residues, so any exact
 //             construction equals fp_twiddles, :173-186)
@@ -667,20 +671,12 @@ __device__ __forceinline__ Tiles make_tiles(double* s, int stride, int ntiles, i
 }
 
 // ---------------------------------------------------------------------------
-// Forward pass of one tile of one operand, both primes (tiles X0, X1).
-// MINB: CTAs per SM the register budget is cut for (3: 80 registers, 4: 64);
-// launches pick 4 when the tile set is small enough for four CTAs' shared memory.
-template <int MINB, bool ODD>
-__global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restrict__ prods,
-                                                         const DPlan* __restrict__ plans,
-                                                         const Job* __restrict__ jobs, int64_t njobs) {
-    extern __shared__ double smem[];
-    // a run of consecutive jobs per CTA: in column passes they share twiddle
-    // columns, which stay in L1 from one tile to the next
-    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
-    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
-    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
-        const Job jb = jobs[ji];
+// Forward pass of one tile of one operand, both primes (tiles X0, X1): one
+// job, run by the whole CTA (the per-kind kernels and the queue kernel call it).
+template <bool ODD>
+__device__ __forceinline__ void job_fwd(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
+                                        const Job& jb, double* smem) {
+    {
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int opb = (jb.sub >> 1) & 1, pass = (jb.sub >> 8) & 0xff;
@@ -708,18 +704,29 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restr
     }
 }
 
+// MINB: CTAs per SM the register budget is cut for (3: 80 registers, 4: 64);
+// launches pick 4 when the tile set is small enough for four CTAs' shared memory.
+template <int MINB, bool ODD>
+__global__ void __launch_bounds__(PASS_THREADS, MINB) k_fwd(const DProd* __restrict__ prods,
+                                                         const DPlan* __restrict__ plans,
+                                                         const Job* __restrict__ jobs, int64_t njobs) {
+    extern __shared__ double smem[];
+    // a run of consecutive jobs per CTA: in column passes they share twiddle
+    // columns, which stay in L1 from one tile to the next
+    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
+    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
+    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) job_fwd<ODD>(prods, plans, jobs[ji], smem);
+}
+
 // Last pass, both primes: forward on a (and b), pointwise, reverse on a.
 // Tiles: products [a0, b0, a1, b1], squares [a0, a1].
 // SPLIT: one CTA per prime (JK_PWR_SPLIT).  KEEPB: launches of products with
 // a kept operand spectrum (JK_PWR_KEEP; PF_BSAVE / PF_BSPEC), compiled apart
 // so the other launches carry none of that code.
 template <bool SPLIT, bool KEEPB, bool ODD>
-__global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd* __restrict__ prods,
-                                                         const DPlan* __restrict__ plans,
-                                                         const Job* __restrict__ jobs, int64_t njobs) {
-    extern __shared__ double smem[];
-    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const Job jb = jobs[ji];
+__device__ __forceinline__ void job_pwr(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
+                                        const Job& jb, double* smem) {
+    {
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int pass = P.npass - 1;
@@ -822,18 +829,19 @@ __global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd*
     }
 }
 
-// Reverse pass of one tile, both primes.
-template <int MINB, bool ODD>
-__global__ void __launch_bounds__(PASS_THREADS, MINB) k_rev(const DProd* __restrict__ prods,
+template <bool SPLIT, bool KEEPB, bool ODD>
+__global__ void __launch_bounds__(PASS_THREADS, NBG_PWR_MINB) k_pwr(const DProd* __restrict__ prods,
                                                          const DPlan* __restrict__ plans,
                                                          const Job* __restrict__ jobs, int64_t njobs) {
     extern __shared__ double smem[];
-    // a run of consecutive jobs per CTA: in column passes they share twiddle
-    // columns, which stay in L1 from one tile to the next
-    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
-    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
-    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
-        const Job jb = jobs[ji];
+    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) job_pwr<SPLIT, KEEPB, ODD>(prods, plans, jobs[ji], smem);
+}
+
+// Reverse pass of one tile, both primes (one job).
+template <bool ODD>
+__device__ __forceinline__ void job_rev(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
+                                        const Job& jb, double* smem) {
+    {
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int pass = (jb.sub >> 8) & 0xff;
@@ -850,6 +858,18 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_rev(const DProd* __restr
         store_tile(smem, P.xa[0], ps, base);
         store_tile(smem + stride, P.xa[1], ps, base);
     }
+}
+
+template <int MINB, bool ODD>
+__global__ void __launch_bounds__(PASS_THREADS, MINB) k_rev(const DProd* __restrict__ prods,
+                                                         const DPlan* __restrict__ plans,
+                                                         const Job* __restrict__ jobs, int64_t njobs) {
+    extern __shared__ double smem[];
+    // a run of consecutive jobs per CTA: in column passes they share twiddle
+    // columns, which stay in L1 from one tile to the next
+    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
+    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
+    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) job_rev<ODD>(prods, plans, jobs[ji], smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -942,20 +962,13 @@ __device__ __forceinline__ void tile_box(const DPass& ps, int64_t t, int& x, int
 
 // One column pass (forward or reverse) of one tile of one operand, both primes,
 // staged by TMA.  Dynamic shared memory: [mbarrier | 120 B | tiles].
-template <int MINB, bool FWD, bool ODD>
-__global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __restrict__ prods,
-                                                             const DPlan* __restrict__ plans,
-                                                             const Job* __restrict__ jobs, int64_t njobs) {
-    extern __shared__ __align__(128) double dsm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm);
-    double* smem = dsm + 16;  // tiles start 128 bytes in
-    if (threadIdx.x == 0) tma::bar_init(bar);
-    __syncthreads();
-    uint32_t phase = 0;
-    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
-    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
-    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++) {
-        const Job jb = jobs[ji];
+// One tile (one job); false when the bounded wait for its load gave up.
+// smem: the tile region (128-byte aligned); bar: the CTA's mbarrier, whose
+// phase the caller keeps.
+template <bool FWD, bool ODD>
+__device__ __forceinline__ bool job_col_tma(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
+                                            const Job& jb, double* smem, uint64_t* bar, uint32_t& phase) {
+    {
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
         const int opb = FWD ? (jb.sub >> 1) & 1 : 0;
@@ -982,10 +995,7 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __r
             if (opb) pack_tile2<false>(smem, smem + cnt, P.b, P.n, P.bch, P.ncb, ps, base);
             else pack_tile2<false>(smem, smem + cnt, P.a, P.m, P.bch, P.nca, ps, base);
         } else {
-            if (!tma::bar_wait(bar, phase)) {  // gave up: leave after the stores issued so far
-                if (threadIdx.x == 0) tma::stores_done();
-                return;
-            }
+            if (!tma::bar_wait(bar, phase)) return false;
             phase ^= 1u;
         }
         run_pass<FWD, false, ODD>(make_tiles(smem, cnt, 2, 0, ps, x), pl, ps);
@@ -993,7 +1003,24 @@ __global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __r
         __syncthreads();
         if (threadIdx.x == 0) tma::store3(map, x, y, z, smem);
     }
-    if (threadIdx.x == 0) tma::stores_done();
+    return true;
+}
+
+template <int MINB, bool FWD, bool ODD>
+__global__ void __launch_bounds__(PASS_THREADS, MINB) k_col_tma(const DProd* __restrict__ prods,
+                                                             const DPlan* __restrict__ plans,
+                                                             const Job* __restrict__ jobs, int64_t njobs) {
+    extern __shared__ __align__(128) double dsm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm);
+    double* smem = dsm + 16;  // tiles start 128 bytes in
+    if (threadIdx.x == 0) tma::bar_init(bar);
+    __syncthreads();
+    uint32_t phase = 0;
+    const int64_t run = (njobs + gridDim.x - 1) / gridDim.x;
+    const int64_t jend = min(njobs, ((int64_t)blockIdx.x + 1) * run);
+    for (int64_t ji = (int64_t)blockIdx.x * run; ji < jend; ji++)
+        if (!job_col_tma<FWD, ODD>(prods, plans, jobs[ji], smem, bar, phase)) break;  // gave up (counted)
+    if (threadIdx.x == 0) tma::stores_done();  // leave after the stores issued so far
 }
 
 // ---------------------------------------------------------------------------
@@ -1132,6 +1159,141 @@ __device__ __forceinline__ void unpack_issue(const DProd& P, int64_t N, const UT
     tma::load1(st2, reinterpret_cast<const void*>(src[1]), bytes[1], bar);
 }
 
+// Phases after the tile's residues are staged (st1, st2: prime 1 and 2, each
+// run starting `lead` doubles in): Garner in place, the per-thread limb
+// windows, the spill exchange, the block carry-lookahead scan, the limb
+// stores and the tile aggregate.  The stage's last read (and write) comes
+// before a block barrier inside, after a proxy fence, so a bulk copy issued
+// after this returns may refill it.
+__device__ __forceinline__ void unpack_assemble(const DProd& P, const DPlan& pl, const Job& jb, const UTile& g,
+                                                double* st1, double* st2, uint32_t* wagg, uint64_t (*spill)[2]) {
+    const int t = threadIdx.x;
+    const int b = P.bch;
+    const int64_t N = pl.N;
+    const int nc = (int)g.ncoef;
+    const int top1 = stage_lead(P.xa[0], N, g) + nc - 1;
+    const int top2 = stage_lead(P.xa[1], N, g) + nc - 1;
+    uint64_t* const u1 = reinterpret_cast<uint64_t*>(st1);
+    uint64_t* const u2 = reinterpret_cast<uint64_t*>(st2);
+    // Garner in place: coefficient k's two residues become its (lo, hi)
+    for (int k0 = t; k0 < nc; k0 += 8 * UNPACK_THREADS) {
+        double a1[8], a2[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int k = k0 + q * UNPACK_THREADS;
+            a1[q] = 0.0;
+            a2[q] = 0.0;
+            if (k < nc) {
+                if (k == 0 && g.ilo == 0) {
+                    a1[q] = P.xa[0][0];  // plain loads: in the queue kernel this launch wrote them
+                    a2[q] = P.xa[1][0];
+                } else {
+                    a1[q] = st1[top1 - k];
+                    a2[q] = st2[top2 - k];
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int k = k0 + q * UNPACK_THREADS;
+            if (k < nc) {
+                uint64_t lo, hi;
+                garner_xy(a1[q], a2[q], pl, lo, hi);
+                u1[top1 - k] = lo;
+                u2[top2 - k] = hi;
+            }
+        }
+    }
+    __syncthreads();
+    const int64_t w0 = g.w0, w1 = g.w1, ilo = g.ilo, ihi = g.ihi;
+    const double rb = 1.0 / (double)b;
+    const int64_t wt = w0 + 4 * (int64_t)t;
+    uint64_t own[4], s0, s1;
+    {
+        const int64_t i0 = div_b(64 * wt + b - 1, b, rb);
+        const int64_t i1 = min(div_b(64 * (wt + 4) - 1, b, rb), ihi);
+        range_limbs<true>(u1, u2, top1, top2, (int)(i0 - ilo), (int)(i1 - ilo), (uint32_t)(b * i0 - 64 * wt),
+                          (uint32_t)b, own, s0, s1);
+    }
+    spill[t + 1][0] = s0;
+    spill[t + 1][1] = s1;
+    if (t == 0) {
+        uint64_t p0 = 0, p1 = 0;
+        if (w0 > 0) {  // the spill of the range [w0 - 4, w0) into limbs w0, w0 + 1
+            const int64_t i1 = min(div_b(64 * w0 - 1, b, rb), ihi);
+            range_limbs<false>(u1, u2, top1, top2, 0, (int)(i1 - ilo), (uint32_t)(b * ilo - 64 * g.wlo),
+                               (uint32_t)b, nullptr, p0, p1);
+        }
+        spill[0][0] = p0;
+        spill[0][1] = p1;
+    }
+    // this stage's generic-proxy accesses come before the bulk copy that
+    // refills it (issued after the barrier below)
+    tma::fence_async();
+    __syncthreads();
+    // own + the spill from below: a carry (0 or 1) out of the 4 limbs, then
+    // generate / propagate across threads
+    uint32_t gen;
+    {
+        const uint64_t a0 = spill[t][0], a1 = spill[t][1];
+        uint32_t c;
+        asm("add.cc.u64 %0, %0, %5;\n\t"
+            "addc.cc.u64 %1, %1, %6;\n\t"
+            "addc.cc.u64 %2, %2, %7;\n\t"
+            "addc.cc.u64 %3, %3, %7;\n\t"
+            "addc.u32 %4, %8, %8;"
+            : "+l"(own[0]), "+l"(own[1]), "+l"(own[2]), "+l"(own[3]), "=r"(c)
+            : "l"(a0), "l"(a1), "l"(0ULL), "r"(0u));
+        gen = c;
+    }
+    // limbs past the product's end are zero and must not propagate
+    uint32_t prop = 1u;
+#pragma unroll
+    for (int q = 0; q < 4; q++) prop &= (wt + q < w1 && own[q] == ~0ULL) ? 1u : 0u;
+    const uint32_t agg = gen | (prop << 1);
+    // block exclusive scan of agg (carry-in to each thread, tile carry-in 0)
+    const int lane = t & 31, wid = t >> 5;
+    uint32_t incl = agg;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = gp_compose(o, incl);
+    }
+    if (lane == 31) wagg[wid] = incl;
+    __syncthreads();
+    uint32_t wpre = 2u;
+    for (int k = 0; k < wid; k++) wpre = gp_compose(wpre, wagg[k]);
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = 2u;
+    excl = gp_compose(wpre, excl);
+    const uint64_t cin = excl & 1u;  // tile carry-in assumed 0
+    asm("add.cc.u64 %0, %0, %4;\n\t"
+        "addc.cc.u64 %1, %1, %5;\n\t"
+        "addc.cc.u64 %2, %2, %5;\n\t"
+        "addc.u64 %3, %3, %5;"
+        : "+l"(own[0]), "+l"(own[1]), "+l"(own[2]), "+l"(own[3])
+        : "l"(cin), "l"(0ULL));
+    if (wt + 3 < w1) {
+        ulonglong2* dst = reinterpret_cast<ulonglong2*>(P.r + wt);
+        if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+            dst[0] = make_ulonglong2(own[0], own[1]);
+            dst[1] = make_ulonglong2(own[2], own[3]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; q++) P.r[wt + q] = own[q];
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (wt + q < w1) P.r[wt + q] = own[q];
+    }
+    if (t == blockDim.x - 1 && P.agg) {
+        uint32_t tot = 2u;
+        for (int k = 0; k < UNPACK_THREADS / 32; k++) tot = gp_compose(tot, wagg[k]);
+        P.agg[jb.tile] = tot;
+    }
+}
+
 // Persistent: CTA c assembles tiles c, c + G, c + 2G, ... (G = gridDim.x); the
 // next tile's residues are in flight (bulk copy into the other stage) while
 // this one is assembled.  Dynamic shared memory: [2 mbarriers | 112 B |
@@ -1161,7 +1323,6 @@ __global__ void __launch_bounds__(UNPACK_THREADS, 3) k_unpack(const DProd* __res
         const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         const DPlan& pl = plans[P.plan];
-        const int b = P.bch;
         const int64_t N = pl.N;
         const UTile g = unpack_tile(P, jb.tile);
         const int64_t jn = ji + gridDim.x;
@@ -1179,183 +1340,79 @@ __global__ void __launch_bounds__(UNPACK_THREADS, 3) k_unpack(const DProd* __res
             if (jn < njobs) tma::bar_wait(bar + (s ^ 1), (uint32_t)((j + 1) >> 1) & 1u);
             return;
         }
-        const int nc = (int)g.ncoef;
-        const int top1 = stage_lead(P.xa[0], N, g) + nc - 1;
-        const int top2 = stage_lead(P.xa[1], N, g) + nc - 1;
-        uint64_t* const u1 = reinterpret_cast<uint64_t*>(st1);
-        uint64_t* const u2 = reinterpret_cast<uint64_t*>(st2);
-        // Garner in place: coefficient k's two residues become its (lo, hi)
-        for (int k0 = t; k0 < nc; k0 += 8 * UNPACK_THREADS) {
-            double a1[8], a2[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const int k = k0 + q * UNPACK_THREADS;
-                a1[q] = 0.0;
-                a2[q] = 0.0;
-                if (k < nc) {
-                    if (k == 0 && g.ilo == 0) {
-                        a1[q] = __ldg(P.xa[0]);
-                        a2[q] = __ldg(P.xa[1]);
-                    } else {
-                        a1[q] = st1[top1 - k];
-                        a2[q] = st2[top2 - k];
-                    }
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const int k = k0 + q * UNPACK_THREADS;
-                if (k < nc) {
-                    uint64_t lo, hi;
-                    garner_xy(a1[q], a2[q], pl, lo, hi);
-                    u1[top1 - k] = lo;
-                    u2[top2 - k] = hi;
-                }
-            }
-        }
-        __syncthreads();
-        const int64_t w0 = g.w0, w1 = g.w1, ilo = g.ilo, ihi = g.ihi;
-        const double rb = 1.0 / (double)b;
-        const int64_t wt = w0 + 4 * (int64_t)t;
-        uint64_t own[4], s0, s1;
-        {
-            const int64_t i0 = div_b(64 * wt + b - 1, b, rb);
-            const int64_t i1 = min(div_b(64 * (wt + 4) - 1, b, rb), ihi);
-            range_limbs<true>(u1, u2, top1, top2, (int)(i0 - ilo), (int)(i1 - ilo), (uint32_t)(b * i0 - 64 * wt),
-                              (uint32_t)b, own, s0, s1);
-        }
-        spill[t + 1][0] = s0;
-        spill[t + 1][1] = s1;
-        if (t == 0) {
-            uint64_t p0 = 0, p1 = 0;
-            if (w0 > 0) {  // the spill of the range [w0 - 4, w0) into limbs w0, w0 + 1
-                const int64_t i1 = min(div_b(64 * w0 - 1, b, rb), ihi);
-                range_limbs<false>(u1, u2, top1, top2, 0, (int)(i1 - ilo), (uint32_t)(b * ilo - 64 * g.wlo),
-                                   (uint32_t)b, nullptr, p0, p1);
-            }
-            spill[0][0] = p0;
-            spill[0][1] = p1;
-        }
-        // this stage's generic-proxy accesses come before the bulk copy that
-        // refills it (issued after the barrier below)
-        tma::fence_async();
-        __syncthreads();
-        // own + the spill from below: a carry (0 or 1) out of the 4 limbs, then
-        // generate / propagate across threads
-        uint32_t gen;
-        {
-            const uint64_t a0 = spill[t][0], a1 = spill[t][1];
-            uint32_t c;
-            asm("add.cc.u64 %0, %0, %5;\n\t"
-                "addc.cc.u64 %1, %1, %6;\n\t"
-                "addc.cc.u64 %2, %2, %7;\n\t"
-                "addc.cc.u64 %3, %3, %7;\n\t"
-                "addc.u32 %4, %8, %8;"
-                : "+l"(own[0]), "+l"(own[1]), "+l"(own[2]), "+l"(own[3]), "=r"(c)
-                : "l"(a0), "l"(a1), "l"(0ULL), "r"(0u));
-            gen = c;
-        }
-        // limbs past the product's end are zero and must not propagate
-        uint32_t prop = 1u;
-#pragma unroll
-        for (int q = 0; q < 4; q++) prop &= (wt + q < w1 && own[q] == ~0ULL) ? 1u : 0u;
-        const uint32_t agg = gen | (prop << 1);
-        // block exclusive scan of agg (carry-in to each thread, tile carry-in 0)
-        const int lane = t & 31, wid = t >> 5;
-        uint32_t incl = agg;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
-            if (lane >= off) incl = gp_compose(o, incl);
-        }
-        if (lane == 31) wagg[wid] = incl;
-        __syncthreads();
-        uint32_t wpre = 2u;
-        for (int k = 0; k < wid; k++) wpre = gp_compose(wpre, wagg[k]);
-        uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) excl = 2u;
-        excl = gp_compose(wpre, excl);
-        const uint64_t cin = excl & 1u;  // tile carry-in assumed 0
-        asm("add.cc.u64 %0, %0, %4;\n\t"
-            "addc.cc.u64 %1, %1, %5;\n\t"
-            "addc.cc.u64 %2, %2, %5;\n\t"
-            "addc.u64 %3, %3, %5;"
-            : "+l"(own[0]), "+l"(own[1]), "+l"(own[2]), "+l"(own[3])
-            : "l"(cin), "l"(0ULL));
-        if (wt + 3 < w1) {
-            ulonglong2* dst = reinterpret_cast<ulonglong2*>(P.r + wt);
-            if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
-                dst[0] = make_ulonglong2(own[0], own[1]);
-                dst[1] = make_ulonglong2(own[2], own[3]);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 4; q++) P.r[wt + q] = own[q];
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (wt + q < w1) P.r[wt + q] = own[q];
-        }
-        if (t == blockDim.x - 1 && P.agg) {
-            uint32_t tot = 2u;
-            for (int k = 0; k < UNPACK_THREADS / 32; k++) tot = gp_compose(tot, wagg[k]);
-            P.agg[jb.tile] = tot;
-        }
+        unpack_assemble(P, pl, jb, g, st1, st2, wagg, spill);
     }
 }
 
-// Cross-tile carries: one CTA per product.  Each thread composes a run of
+// Cross-tile carries of one product (one CTA).  Each thread composes a run of
 // tile aggregates, the block scans them, and every tile whose true carry-in is
 // 1 gets +1 propagated from its first limb (limbs equal to 2^64-1 wrap to 0).
+__device__ __forceinline__ void carry_product(const DProd& P, uint32_t* wagg) {
+    const int64_t nt = P.ntl;
+    if (nt <= 1) return;  // one tile: no carry crosses a tile boundary
+    const int t = threadIdx.x;
+    const int64_t per = (nt + blockDim.x - 1) / blockDim.x;
+    const int64_t t0 = (int64_t)t * per, t1 = min(t0 + per, nt);
+    uint32_t agg = 2u;
+    for (int64_t k = t0; k < t1; k++) agg = gp_compose(agg, P.agg[k]);
+    const int lane = t & 31, wid = t >> 5;
+    uint32_t incl = agg;
+    for (int off = 1; off < 32; off <<= 1) {
+        uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = gp_compose(o, incl);
+    }
+    __syncthreads();
+    if (lane == 31) wagg[wid] = incl;
+    __syncthreads();
+    uint32_t wpre = 2u;
+    for (int k = 0; k < wid; k++) wpre = gp_compose(wpre, wagg[k]);
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = 2u;
+    excl = gp_compose(wpre, excl);
+    uint32_t cin = excl & 1u;
+    for (int64_t k = t0; k < t1; k++) {
+        uint32_t a = P.agg[k];
+        if (cin) {
+            // the carry stops at the tile's first limb unless that limb is
+            // all ones; such tiles are flagged for carry_fix_tile, which
+            // walks the run of all-ones limbs with a whole warp
+            const int64_t w = k * UNPACK_TL;
+            if (P.r[w] != ~0ULL) P.r[w] += 1;
+            else P.agg[k] = a | 4u;
+        }
+        cin = (a & 1u) | ((a >> 1) & cin);
+    }
+}
+
 __global__ void __launch_bounds__(256) k_carry(const DProd* __restrict__ prods, const Job* __restrict__ jobs,
                                                int64_t njobs) {
     __shared__ uint32_t wagg[8];
-    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
-        const DProd& P = prods[jobs[ji].prod];
-        const int64_t nt = P.ntl;
-        if (nt <= 1) continue;  // one tile: no carry crosses a tile boundary
-        const int t = threadIdx.x;
-        const int64_t per = (nt + blockDim.x - 1) / blockDim.x;
-        const int64_t t0 = (int64_t)t * per, t1 = min(t0 + per, nt);
-        uint32_t agg = 2u;
-        for (int64_t k = t0; k < t1; k++) agg = gp_compose(agg, P.agg[k]);
-        const int lane = t & 31, wid = t >> 5;
-        uint32_t incl = agg;
-        for (int off = 1; off < 32; off <<= 1) {
-            uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
-            if (lane >= off) incl = gp_compose(o, incl);
+    for (int64_t ji = blockIdx.x; ji < njobs; ji += gridDim.x) carry_product(prods[jobs[ji].prod], wagg);
+}
+
+// A tile that carry_product flagged (bit 2 of its aggregate): the incoming
+// carry runs through the tile's leading all-ones limbs.  One warp: the tile
+// is read 32 limbs at a time until the first limb that is not all ones (it
+// absorbs the +1), the run before it zeroed; a tile that is all ones passes
+// the carry on, which the cross-tile scan already credited to the next tile.
+__device__ __forceinline__ void carry_fix_tile(const DProd& P, int64_t tile, int lane) {
+    const int64_t w0 = tile * UNPACK_TL, we = min(w0 + (int64_t)UNPACK_TL, P.rn);
+    for (int64_t w = w0; w < we; w += 32) {
+        const int64_t wl = w + lane;
+        const uint64_t v = wl < we ? P.r[wl] : 0ULL;  // past the tile: stops the run
+        const unsigned notones = __ballot_sync(0xffffffffu, v != ~0ULL);
+        if (notones) {
+            const int k = __ffs(notones) - 1;
+            if (lane < k) P.r[wl] = 0;
+            else if (lane == k && wl < we) P.r[wl] = v + 1;
+            break;
         }
-        __syncthreads();
-        if (lane == 31) wagg[wid] = incl;
-        __syncthreads();
-        uint32_t wpre = 2u;
-        for (int k = 0; k < wid; k++) wpre = gp_compose(wpre, wagg[k]);
-        uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) excl = 2u;
-        excl = gp_compose(wpre, excl);
-        uint32_t cin = excl & 1u;
-        for (int64_t k = t0; k < t1; k++) {
-            uint32_t a = P.agg[k];
-            if (cin) {
-                // the carry stops at the tile's first limb unless that limb is
-                // all ones; such tiles are left to k_carry_fix, which walks
-                // the run of all-ones limbs with the whole block
-                const int64_t w = k * UNPACK_TL;
-                if (P.r[w] != ~0ULL) P.r[w] += 1;
-                else P.agg[k] = a | 4u;
-            }
-            cin = (a & 1u) | ((a >> 1) & cin);
-        }
+        P.r[wl] = 0;  // all 32 are all ones (and inside the tile)
     }
 }
 
-// Tiles that k_carry flagged (bit 2 of their aggregate): the incoming carry
-// runs through the tile's leading all-ones limbs.  One warp per tile: an
-// unflagged tile is left at once; a flagged one is read 32 limbs at a time
-// until the first limb that is not all ones (it absorbs the +1), the run before
-// it zeroed; a tile that is all ones passes the carry on, which the cross-tile
-// scan already credited to the next tile.  Jobs are the unpack's (product,
-// tile) list.
+// Flagged tiles, one warp per tile (most tiles are left at once).  Jobs are
+// the unpack's (product, tile) list.
 __global__ void __launch_bounds__(256) k_carry_fix(const DProd* __restrict__ prods, const Job* __restrict__ jobs,
                                                    int64_t njobs) {
     const int lane = threadIdx.x & 31;
@@ -1364,19 +1421,299 @@ __global__ void __launch_bounds__(256) k_carry_fix(const DProd* __restrict__ pro
         const Job jb = jobs[ji];
         const DProd& P = prods[jb.prod];
         if (P.ntl <= 1 || !(P.agg[jb.tile] & 4u)) continue;
-        const int64_t w0 = jb.tile * UNPACK_TL, we = min(w0 + (int64_t)UNPACK_TL, P.rn);
-        for (int64_t w = w0; w < we; w += 32) {
-            const int64_t wl = w + lane;
-            const uint64_t v = wl < we ? P.r[wl] : 0ULL;  // past the tile: stops the run
-            const unsigned notones = __ballot_sync(0xffffffffu, v != ~0ULL);
-            if (notones) {
-                const int k = __ffs(notones) - 1;
-                if (lane < k) P.r[wl] = 0;
-                else if (lane == k && wl < we) P.r[wl] = v + 1;
+        carry_fix_tile(P, jb.tile, lane);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Work-queue execution: one persistent launch runs a whole batch.  Each CTA
+// claims the next queue positions (an atomic counter), waits until the job's
+// product has finished its previous pipeline step (per product and step, a
+// count of finished jobs against the count the step has), runs the job and
+// counts it finished.  Positions are claimed in pipeline-step order, so every
+// job a CTA waits for was claimed earlier by a CTA that is running: the
+// earliest unfinished job never waits, and the queue drains.  Waits are
+// bounded: one that gives up counts a fault and raises the abort flag, on
+// which every CTA leaves.
+
+__device__ __forceinline__ int queue_step(int kind, const Job& jb, int npass) {
+    switch (kind) {
+        case JK_FWD:
+        case JK_FWD_TMA: return (jb.sub >> 8) & 0xff;
+        case JK_PWR:
+        case JK_PWR_SPLIT:
+        case JK_PWR_KEEP: return npass - 1;
+        case JK_REV:
+        case JK_REV_TMA: return 2 * npass - 2 - ((jb.sub >> 8) & 0xff);
+        case JK_UNPACK: return 2 * npass - 1;
+        default: return 2 * npass;  // JK_CARRY
+    }
+}
+
+__device__ __forceinline__ int queue_entry(const QLaunch* __restrict__ ql, int nl, int64_t g) {
+    int lo = 0, hi = nl - 1;  // last entry with qstart <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ql[mid].qstart <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ bool queue_aborted(const QState* qs) {
+    return *reinterpret_cast<const volatile unsigned int*>(&qs->abort) != 0u;
+}
+
+// Waits (bounded: about 2^31 SM clocks, a second) until *cnt >= want.
+__device__ __forceinline__ bool queue_wait(const uint32_t* cnt, uint32_t want, QState* qs) {
+    if (ld_acquire(cnt) >= want) return true;
+    const long long t0 = clock64();
+    for (;;) {
+        __nanosleep(100);
+        if (ld_acquire(cnt) >= want) return true;
+        if (queue_aborted(qs)) return false;
+        if (clock64() - t0 > (1LL << 31)) {
+            atomicAdd(&g_nbg_faults, 1u);
+            atomicExch(&qs->abort, 1u);
+            return false;
+        }
+    }
+}
+
+// One unpack tile, its residues staged by bulk copy into `reg` (one stage).
+__device__ __forceinline__ bool job_unpack(const DProd* __restrict__ prods, const DPlan* __restrict__ plans,
+                                           const Job& jb, double* reg, uint64_t* bar, uint32_t& phase,
+                                           uint32_t* wagg, uint64_t (*spill)[2]) {
+    const DProd& P = prods[jb.prod];
+    const DPlan& pl = plans[P.plan];
+    const UTile g = unpack_tile(P, jb.tile);
+    const int cap = (int)unpack_stage_doubles(P.bch);
+    double* const st1 = reg;
+    double* const st2 = reg + cap;
+    if (threadIdx.x == 0) unpack_issue(P, pl.N, g, st1, st2, bar);
+    if (!tma::bar_wait(bar, phase)) return false;
+    phase ^= 1u;
+    unpack_assemble(P, pl, jb, g, st1, st2, wagg, spill);
+    return true;
+}
+
+// The cross-tile carries of one product and the tiles they flag.
+__device__ __forceinline__ void job_carry(const DProd& P, uint32_t* wagg) {
+    if (P.ntl <= 1) return;
+    carry_product(P, wagg);
+    __syncthreads();  // the flags and +1s are written
+    const int lane = threadIdx.x & 31;
+    for (int64_t k0 = (int64_t)(threadIdx.x >> 5) * 32; k0 < P.ntl; k0 += (int64_t)(blockDim.x >> 5) * 32) {
+        const int64_t k = k0 + lane;
+        unsigned f = __ballot_sync(0xffffffffu, k < P.ntl && (P.agg[k] & 4u));
+        for (; f; f &= f - 1) carry_fix_tile(P, k0 + __ffs(f) - 1, lane);
+    }
+}
+
+// Publishes this CTA's finished jobs of one (product, step): their column
+// tiles' bulk stores have landed, and their results are visible before the
+// count that releases them.
+__device__ __forceinline__ void queue_publish(uint32_t* done, int64_t pend_c, uint32_t& pend_n) {
+    if (pend_n == 0) return;
+    tma::stores_done();
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    __threadfence();
+    atomicAdd(done + pend_c, pend_n);
+    pend_n = 0;
+}
+
+// The queue kernel's dynamic shared memory, named at file scope so that the
+// job functions below address it as shared memory without a pointer argument:
+// [mbarrier | 120 B | region].
+extern __shared__ __align__(128) double q_dsm[];
+
+// One job of each kind, each compiled as a function of its own: a job then has
+// the kernel's whole register budget, and only the queue loop's few values are
+// saved around the call.  Column and unpack jobs return the mbarrier phase
+// after the job in bit 0 and success in bit 1.
+template <bool ODD>
+__device__ __noinline__ void qj_fwd(const DProd* __restrict__ prods, const DPlan* __restrict__ plans, Job jb) {
+    job_fwd<ODD>(prods, plans, jb, q_dsm + 16);
+}
+template <bool ODD>
+__device__ __noinline__ void qj_rev(const DProd* __restrict__ prods, const DPlan* __restrict__ plans, Job jb) {
+    job_rev<ODD>(prods, plans, jb, q_dsm + 16);
+}
+template <bool SPLIT, bool KEEPB, bool ODD>
+__device__ __noinline__ void qj_pwr(const DProd* __restrict__ prods, const DPlan* __restrict__ plans, Job jb) {
+    job_pwr<SPLIT, KEEPB, ODD>(prods, plans, jb, q_dsm + 16);
+}
+template <bool FWD, bool ODD>
+__device__ __noinline__ uint32_t qj_col(const DProd* __restrict__ prods, const DPlan* __restrict__ plans, Job jb,
+                                        uint32_t phase) {
+    const bool ok = job_col_tma<FWD, ODD>(prods, plans, jb, q_dsm + 16, reinterpret_cast<uint64_t*>(q_dsm), phase);
+    return (phase & 1u) | (ok ? 2u : 0u);
+}
+__device__ __noinline__ uint32_t qj_unpack(const DProd* __restrict__ prods, const DPlan* __restrict__ plans, Job jb,
+                                           uint32_t phase) {
+    __shared__ uint32_t wagg[UNPACK_THREADS / 32];
+    __shared__ uint64_t spill[UNPACK_THREADS + 1][2];
+    const bool ok = job_unpack(prods, plans, jb, q_dsm + 16, reinterpret_cast<uint64_t*>(q_dsm), phase, wagg, spill);
+    return (phase & 1u) | (ok ? 2u : 0u);
+}
+__device__ __noinline__ void qj_carry(const DProd* __restrict__ prods, Job jb) {
+    __shared__ uint32_t wagg[UNPACK_THREADS / 32];
+    job_carry(prods[jb.prod], wagg);
+}
+
+// The region holds the largest tile set of the batch's launches and one
+// unpack stage.  A CTA
+// claims `chunk` consecutive queue positions at a time (one atomic); thread 0
+// checks each job's dependency (an acquire only when the count it needs was
+// not seen complete before) and publishes finished jobs in runs of one
+// (product, step), always before it waits, so no CTA waits on a count that
+// a waiting CTA holds back.
+__global__ void __launch_bounds__(PASS_THREADS, 3) k_queue(const DProd* __restrict__ prods,
+                                                          const DPlan* __restrict__ plans,
+                                                          const Job* __restrict__ jobs,
+                                                          const QLaunch* __restrict__ ql, int nl, QState* qs,
+                                                          uint32_t* done, const uint32_t* __restrict__ need,
+                                                          int chunk) {
+    __shared__ int64_t s_g;
+    __shared__ int s_n, s_k, s_ok;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(q_dsm);
+    const int t = threadIdx.x;
+    if (t == 0) tma::bar_init(bar);
+    __syncthreads();
+    uint32_t phase = 0;
+    const int64_t total = ql[nl].qstart;
+    // thread 0: the (product, step) counter of finished, unpublished jobs, and
+    // the last dependency counter seen complete
+    int64_t pend_c = -1, seen_c = -1;
+    uint32_t pend_n = 0;
+    int k = 0;
+    for (;;) {
+        if (t == 0) {
+            int64_t g = -1;
+            int n = 0;
+            if (!queue_aborted(qs)) {
+                g = (int64_t)atomicAdd(&qs->head, (unsigned long long)chunk);
+                if (g < total) {
+                    n = (int)min((int64_t)chunk, total - g);
+                    k = queue_entry(ql, nl, g);
+                } else {
+                    g = -1;
+                }
+            }
+            s_g = g;
+            s_n = n;
+        }
+        __syncthreads();
+        const int64_t g0 = s_g;
+        const int n = s_n;
+        if (g0 < 0) break;
+        bool ok = true;
+        for (int i = 0; i < n; i++) {
+            const int64_t g = g0 + i;
+            if (t == 0) {
+                while (ql[k + 1].qstart <= g) k++;
+                const Job jq = jobs[ql[k].off + (g - ql[k].qstart)];
+                const int st = queue_step(ql[k].kind, jq, prods[jq.prod].npass);
+                int good = 1;
+                if (st > 0) {
+                    const int64_t c = (int64_t)jq.prod * QSTEPS + st - 1;
+                    if (c != seen_c) {
+                        if (ld_acquire(done + c) < need[c]) {
+                            queue_publish(done, pend_c, pend_n);  // never wait holding finished jobs back
+                            good = queue_wait(done + c, need[c], qs) ? 1 : 0;
+                        }
+                        seen_c = c;
+                    }
+                }
+                // the previous job's bulk store has read shared memory, and what
+                // the acquire made visible is visible to this job's bulk loads
+                tma::stores_read();
+                asm volatile("fence.proxy.async.global;" ::: "memory");
+                s_k = k;
+                s_ok = good;
+            }
+            __syncthreads();
+            if (!s_ok) {
+                ok = false;
                 break;
             }
-            P.r[wl] = 0;  // all 32 are all ones (and inside the tile)
+            const QLaunch L = ql[s_k];
+            const Job jb = jobs[L.off + (g - L.qstart)];
+            uint32_t r = 2u | phase;
+            const bool odd = L.odd != 0;
+            switch (L.kind) {
+                case JK_FWD:
+                    if (odd) qj_fwd<true>(prods, plans, jb);
+                    else qj_fwd<false>(prods, plans, jb);
+                    break;
+                case JK_FWD_TMA:
+                    r = odd ? qj_col<true, true>(prods, plans, jb, phase) : qj_col<true, false>(prods, plans, jb, phase);
+                    break;
+                case JK_PWR:
+                    if (odd) qj_pwr<false, false, true>(prods, plans, jb);
+                    else qj_pwr<false, false, false>(prods, plans, jb);
+                    break;
+                case JK_PWR_SPLIT:
+                    if (odd) qj_pwr<true, false, true>(prods, plans, jb);
+                    else qj_pwr<true, false, false>(prods, plans, jb);
+                    break;
+                case JK_PWR_KEEP:
+                    if (odd) qj_pwr<false, true, true>(prods, plans, jb);
+                    else qj_pwr<false, true, false>(prods, plans, jb);
+                    break;
+                case JK_REV:
+                    if (odd) qj_rev<true>(prods, plans, jb);
+                    else qj_rev<false>(prods, plans, jb);
+                    break;
+                case JK_REV_TMA:
+                    r = odd ? qj_col<false, true>(prods, plans, jb, phase)
+                            : qj_col<false, false>(prods, plans, jb, phase);
+                    break;
+                case JK_UNPACK: r = qj_unpack(prods, plans, jb, phase); break;
+                case JK_CARRY: qj_carry(prods, jb); break;
+                default: break;
+            }
+            phase = r & 1u;
+            ok = (r & 2u) != 0;
+            // this job's generic shared-memory accesses come before the next
+            // job's bulk copies into the region; every thread's stores are issued
+            tma::fence_async();
+            ok = __syncthreads_and(ok) != 0;
+            if (!ok) break;
+            if (t == 0) {
+                const int64_t c = (int64_t)jb.prod * QSTEPS + queue_step(L.kind, jb, prods[jb.prod].npass);
+                if (c != pend_c) {
+                    queue_publish(done, pend_c, pend_n);
+                    pend_c = c;
+                }
+                pend_n++;
+            }
         }
+        if (!ok) {
+            if (t == 0) atomicExch(&qs->abort, 1u);
+            break;
+        }
+        if (t == 0) queue_publish(done, pend_c, pend_n);
+    }
+    if (t == 0) tma::stores_done();
+}
+
+// need[prod * QSTEPS + step] += 1 for every queued job.
+__global__ void k_qcount(const DProd* __restrict__ prods, const Job* __restrict__ jobs,
+                         const QLaunch* __restrict__ ql, int nl, uint32_t* need) {
+    const int64_t total = ql[nl].qstart;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int k = queue_entry(ql, nl, g);
+        const Job jb = jobs[ql[k].off + (g - ql[k].qstart)];
+        const int s = queue_step(ql[k].kind, jb, prods[jb.prod].npass);
+        atomicAdd(need + (size_t)jb.prod * QSTEPS + s, 1u);
     }
 }
 
@@ -1462,7 +1799,8 @@ cudaError_t kernels_init(double p1, double p2) {
                         (const void*)k_col_tma<3, true, true>, (const void*)k_col_tma<4, true, true>,
                         (const void*)k_col_tma<3, false, true>, (const void*)k_col_tma<4, false, true>,
                         (const void*)k_col_tma<3, true, false>, (const void*)k_col_tma<4, true, false>,
-                        (const void*)k_col_tma<3, false, false>, (const void*)k_col_tma<4, false, false>};
+                        (const void*)k_col_tma<3, false, false>, (const void*)k_col_tma<4, false, false>,
+                        (const void*)k_queue};
     for (const void* k : ks) {
         cudaFuncAttributes fa;
         e = cudaFuncGetAttributes(&fa, k);
@@ -1557,6 +1895,29 @@ cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const 
         default: return cudaErrorInvalidValue;
     }
 #undef NBG_ODD
+    return cudaGetLastError();
+}
+
+cudaError_t launch_qcount(const DProd* prods, const Job* jobs, const QLaunch* ql, int nl, int64_t total,
+                          uint32_t* need, cudaStream_t st) {
+    if (total <= 0) return cudaSuccess;
+    const unsigned grid = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 8);
+    k_qcount<<<grid, 256, 0, st>>>(prods, jobs, ql, nl, need);
+    return cudaGetLastError();
+}
+
+cudaError_t queue_grid(size_t smem, int* grid) {
+    int nb = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_queue, PASS_THREADS, smem);
+    if (e != cudaSuccess) return e;
+    *grid = std::max(nb, 1) * g_num_sms.load();
+    return cudaSuccess;
+}
+
+cudaError_t launch_queue(const DProd* prods, const DPlan* plans, const Job* jobs, const QLaunch* ql, int nl,
+                         QState* qs, uint32_t* done, const uint32_t* need, size_t smem, int grid, int chunk,
+                         cudaStream_t st) {
+    k_queue<<<(unsigned)grid, PASS_THREADS, smem, st>>>(prods, plans, jobs, ql, nl, qs, done, need, chunk);
     return cudaGetLastError();
 }
 

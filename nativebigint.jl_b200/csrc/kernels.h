@@ -27,6 +27,17 @@ inline JobSrc job_list(const Job* l) {
 cudaError_t launch_jobs(int kind, const DProd* prods, const DPlan* plans, const JobSrc& jobs, int64_t njobs,
                         size_t smem, int grid_cap, cudaStream_t st, bool odd = true);
 
+// Work-queue execution of a batch (k_queue): need[prod * QSTEPS + step] +=
+// the jobs of every step (need zeroed first), the persistent grid for a
+// dynamic shared-memory size, and the launch (qs and done zeroed first) whose
+// CTAs claim `chunk` consecutive jobs at a time.
+cudaError_t launch_qcount(const DProd* prods, const Job* jobs, const QLaunch* ql, int nl, int64_t total,
+                          uint32_t* need, cudaStream_t st);
+cudaError_t queue_grid(size_t smem, int* grid);
+cudaError_t launch_queue(const DProd* prods, const DPlan* plans, const Job* jobs, const QLaunch* ql, int nl,
+                         QState* qs, uint32_t* done, const uint32_t* need, size_t smem, int grid, int chunk,
+                         cudaStream_t st);
+
 // Writes a batch's explicit job list from its compact description: out[g] for
 // every g < total, entry e covering [e.begin, e.begin + e.n).
 cudaError_t launch_expand(const ExpandEntry* entries, int nentries, Job* out, int64_t total, cudaStream_t st);

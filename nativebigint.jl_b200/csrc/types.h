@@ -93,6 +93,27 @@ struct Job {
     int64_t tile;
 };
 
+// Work-queue execution of a batch (one persistent launch): the batch's
+// launches, in pipeline-step order, as consecutive ranges of queue positions.
+// Queue position g lies in entry k when qstart[k] <= g < qstart[k + 1]; its
+// job is jobs[off + g - qstart].  A last entry holds the total in qstart.
+struct QLaunch {
+    int64_t qstart;
+    int64_t off;
+    int32_t kind;  // JobKind (no JK_CARRYFIX: the carry job fixes its own tiles)
+    int32_t odd;
+};
+// Queue state, zeroed before every run.
+struct QState {
+    unsigned long long head;  // next queue position to claim
+    unsigned int abort;       // a bounded wait gave up: every CTA leaves
+    unsigned int pad_;
+};
+// Per product, the jobs of each of its pipeline steps: forward passes
+// 0..npass-2, the last pass (npass-1), reverse passes (npass..2 npass-2),
+// unpack (2 npass-1) and carry (2 npass).
+constexpr int QSTEPS = 2 * MAXPASS + 2;
+
 // A run of jobs of one plan class inside a launch: jobs [begin, begin +
 // ntiles * nop * nprod), ordered tile-major, then operand, then product, so
 // CTAs that run together read the same twiddle slice.  The class's products

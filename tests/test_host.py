@@ -71,11 +71,13 @@ def test_argument_errors_without_device():
 def test_tuning_round_trip():
     old = nbgpu.get_tuning()
     try:
-        nbgpu.set_tuning('{"last_max": 2048, "cmax": 64}')
+        nbgpu.set_tuning('{"last_max": 2048, "cmax": 64, "queue": 4}')
         t = nbgpu.get_tuning()
-        assert '"last_max": 2048' in t and '"cmax": 64' in t
+        assert '"last_max": 2048' in t and '"cmax": 64' in t and '"queue": 4' in t
         with pytest.raises(nbgpu.NBGError):
             nbgpu.set_tuning('{"cmax": 3}')
+        with pytest.raises(nbgpu.NBGError):
+            nbgpu.set_tuning('{"queue": 65}')
     finally:
         nbgpu.set_tuning(old)
     assert nbgpu.get_tuning() == old

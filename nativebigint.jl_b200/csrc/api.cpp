@@ -140,7 +140,10 @@ int host_batch(const nbg_desc* descs, int64_t count) {
     // Each chunk is built on the host while the chunks before it copy and
     // compute; its device region comes from the stream-ordered allocator and
     // goes back after its results are copied out.  At most NBUF chunks are in
-    // flight (the host waits for the oldest before starting another).
+    // flight (the host waits for the oldest before starting another).  A
+    // chunk's launches of one pipeline step run on parallel streams (a chunk
+    // holds a tenth of a large batch, so one step's launches are small and
+    // their tails overlap): 10,000 mixed products 45.6 -> 40.9 ms.
     cudaEvent_t ev_in[NBUF], ev_comp[NBUF], ev_out[NBUF];
     for (int i = 0; i < NBUF; i++) {
         CUDA_TRY(cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming));
@@ -219,7 +222,7 @@ int host_batch(const nbg_desc* descs, int64_t count) {
             if (crc) break;
             cudaEventRecord(ev_in[buf], E.copy_in);
             cudaStreamWaitEvent(E.stream, ev_in[buf], 0);
-            if ((crc = run_launches(E, c.bb, base, E.stream))) break;
+            if ((crc = run_launches_branched(E, c.bb, base, E.stream, E.side, 4))) break;
             cudaEventRecord(ev_comp[buf], E.stream);
             cudaStreamWaitEvent(E.copy_out, ev_comp[buf], 0);
             for (const Span& sp : c.out_spans)

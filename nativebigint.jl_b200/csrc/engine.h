@@ -80,6 +80,12 @@ struct Engine {
     // pinned staging for the descriptor/job-table head of each pipelined chunk
     char* stage[4] = {};
     size_t stage_bytes[4] = {};
+    // pinned staging of operands and results that live in pageable host
+    // memory (host-buffer batches), per pipeline slot; allocated on first need
+    char* pg_in[4] = {};
+    size_t pg_in_bytes[4] = {};
+    char* pg_out[4] = {};
+    size_t pg_out_bytes[4] = {};
 
     int init(int device);
     int ensure();

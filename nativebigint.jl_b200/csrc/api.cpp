@@ -65,6 +65,8 @@ namespace {
 
 constexpr size_t CHUNK_BYTES = size_t(128) << 20;
 constexpr int NBUF = 3;
+// chunks with fewer operand and result bytes copy pageable spans directly
+constexpr size_t STAGE_MIN_BYTES = size_t(8) << 20;
 
 struct Span {
     const char* h;  // host start
@@ -269,14 +271,14 @@ int host_batch(const nbg_desc* descs, int64_t count) {
     // flight (the host waits for the oldest before starting another).  A
     // chunk's launches of one pipeline step run on parallel streams (a chunk
     // holds a tenth of a large batch, so one step's launches are small and
-    // their tails overlap): 10,000 mixed products 45.6 -> 40.9 ms.
-    cudaEvent_t ev_in[NBUF], ev_comp[NBUF], ev_out[NBUF];
+    // their tails overlap): 10,000 mixed products 45.6 -> 40.9 ms.  The
+    // per-slot events are the engine's (host calls are serialized by the API
+    // lock).
+    static_assert(NBUF <= 4, "the engine keeps 4 event slots");
+    cudaEvent_t* ev_in = E.hb_ev[0];
+    cudaEvent_t* ev_comp = E.hb_ev[1];
+    cudaEvent_t* ev_out = E.hb_ev[2];
     PendingOut pend[NBUF];  // per slot: the last chunk's results staged for pageable memory
-    for (int i = 0; i < NBUF; i++) {
-        CUDA_TRY(cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming));
-        CUDA_TRY(cudaEventCreateWithFlags(&ev_comp[i], cudaEventDisableTiming));
-        CUDA_TRY(cudaEventCreateWithFlags(&ev_out[i], cudaEventDisableTiming));
-    }
     {
         // keep freed chunk regions in the device's memory pool for the next call
         // instead of returning them to the driver at each synchronization
@@ -308,13 +310,18 @@ int host_batch(const nbg_desc* descs, int64_t count) {
         std::vector<size_t> ioff, ooff;
         c.in_bytes = layout_spans(ir, 0, c.in_spans, ioff);
         c.out_bytes = layout_spans(orr, 0, c.out_spans, ooff);
+        // small chunks (single products) leave pageable spans to the driver's
+        // own staged copies: checking and staging cost more there (4864-limb
+        // product per call 103 us against 126 us)
         bool any_in_pg = false;
         c.in_pg.assign(c.in_spans.size(), 0);
         c.out_pg.assign(c.out_spans.size(), 0);
-        for (size_t i = 0; i < c.in_spans.size(); i++)
-            if (!dma_ok(c.in_spans[i].h, c.in_spans[i].n)) c.in_pg[i] = 1, any_in_pg = true;
-        for (size_t i = 0; i < c.out_spans.size(); i++)
-            if (!dma_ok(c.out_spans[i].h, c.out_spans[i].n)) c.out_pg[i] = 1, c.any_out_pg = true;
+        if (c.in_bytes + c.out_bytes >= STAGE_MIN_BYTES) {
+            for (size_t i = 0; i < c.in_spans.size(); i++)
+                if (!dma_ok(c.in_spans[i].h, c.in_spans[i].n)) c.in_pg[i] = 1, any_in_pg = true;
+            for (size_t i = 0; i < c.out_spans.size(); i++)
+                if (!dma_ok(c.out_spans[i].h, c.out_spans[i].n)) c.out_pg[i] = 1, c.any_out_pg = true;
+        }
         const size_t base_in = align_up(c.bb.dev_bytes, 256), base_out = base_in + c.in_bytes;
         c.region = align_up(base_out + c.out_bytes, 256);
         // the slot's previous chunk: its staging buffer and its events are reused
@@ -410,11 +417,6 @@ int host_batch(const nbg_desc* descs, int64_t count) {
     cudaError_t e3 = cudaStreamSynchronize(E.copy_out);
     if (rc == NBG_OK && e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess)
         for (int i = 0; i < NBUF; i++) scatter_out(pend[i], E.pg_out[i]);
-    for (int i = 0; i < NBUF; i++) {
-        cudaEventDestroy(ev_in[i]);
-        cudaEventDestroy(ev_comp[i]);
-        cudaEventDestroy(ev_out[i]);
-    }
     if (rc) return rc;
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
         return fail(NBG_ECUDA, "host batch: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3));

@@ -344,6 +344,8 @@ int Engine::init(int device) {
     CUDA_TRY(cudaStreamCreateWithFlags(&copy_in, cudaStreamNonBlocking));
     CUDA_TRY(cudaStreamCreateWithFlags(&copy_out, cudaStreamNonBlocking));
     for (cudaStream_t& s : side) CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    for (auto& row : hb_ev)
+        for (cudaEvent_t& e : row) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CUDA_TRY(kernels_init((double)PR[0], (double)PR[1]));
     CUDA_TRY(cudaMalloc(&d_plans, sizeof(DPlan) * (size_t)plan_cap));
     CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));

@@ -68,6 +68,7 @@ struct Engine {
     cudaStream_t copy_in = nullptr;  // host-to-device copies of the pipelined host calls
     cudaStream_t copy_out = nullptr; // device-to-host copies
     cudaStream_t side[4] = {};       // parallel branches of one pipeline step (host-buffer batches)
+    cudaEvent_t hb_ev[3][4] = {};    // host-buffer batches: per slot, operands in / computed / results out
     std::recursive_mutex mu;
     Tuning tun;
     std::map<int64_t, PlanRec> plans;
